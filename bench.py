@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""Benchmark: MLS-MPM fluid substep + diffuse update, particle-updates/s.
+
+Workload (one "step" = one substep of the scene, all passes incl. diffuse):
+  dam_break_1m — 128^3 grid, 1,048,576 particles (seeded-jitter dam break,
+  block 40% of the width x 60% of the height), diffuse pool 262,144.
+Multi-GPU (torchrun): every rank simulates its own independent scene (seed =
+rank) — scene sharding with no data-path collective; `value` sums all ranks'
+particle-updates over the max-over-ranks device time ("scaling": "weak").
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mls-mpm_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-updates/s @1M (frac HBM roofline)"
+UNIT = "particle-updates/s"
+WORKLOAD = "dam_break_1m"
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured hbm_gbs (MEASURED_PEAKS.json)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+# Algorithmic bytes per unit of each phase (reference vec4/affine9 layouts):
+# per particle: P2G_MASS 20 (pos 16 + mass 4), P2G_MOM 76 (pos 16 + vel 16 +
+# C 36 + mass 4 + density 4), G2P 84 (pos 16 in; pos 16 + vel 16 + C 36 out);
+# per cell: P2G_MASS 4 (mass i32 write), P2G_MOM 16 (mass read 4 + momentum
+# i32 write 12), UPDATE_GRID 28 (momentum+mass read 16, velocity write 12),
+# G2P 12 (velocity read).  Sum: 180 B per particle + 60 B per cell.
+PHASE_BYTES = {"p2g_mass": (20, 4), "p2g_mom": (76, 16), "update_grid": (0, 28), "g2p": (84, 12)}
+
+
+class ClockSampler:
+    """NVML sampling of SM clock and throttle reasons while running."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x1: "gpu_idle", 0x2: "applications_clocks_setting",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._h = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if r & bit and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.01)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self._h is not None:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_reference_rate(scene, substeps, threads, budget_s=None):
+    """Times the reference pin (the reference's WGSL compiled on the host) or,
+    when it is absent, the oracle restatement, over `substeps` substeps of
+    `scene` with diffuse.  Returns (updates/s, kind, steps run, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as O
+    import scenarios
+    kind = "reference" if O.ref_available() else "port"
+    impl = "ref" if kind == "reference" else "oracle"
+    sc = scenarios.Scenario(scene.name, scene, substeps + 1, diffuse_max=scene.diffuse_max)
+    st = O.new_state(scene, scene.diffuse_max)
+    frames = sc.frames()
+    P, W, H, dims, gen, adv = next(frames)
+    O.substep(st, P, W, H, dims, gen, adv, threads=threads, impl=impl)    # warm caches
+    t0 = time.perf_counter()
+    done = 0
+    for P, W, H, dims, gen, adv in frames:
+        O.substep(st, P, W, H, dims, gen, adv, threads=threads, impl=impl)
+        done += 1
+        if budget_s and time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return scene.n * done / dt, kind, done, dt
+
+
+def run_reference_arm(args, ws, rank):
+    from mls_mpm_b200 import scenes
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    scene = scenes.dam_break_1m(0)
+    # warm-up steps are untimed; each timed step is one full substep of the
+    # scene; the run is capped at ~240 s of CPU time (the sample is stated)
+    rate_w, kind, _, _ = cpu_reference_rate(scene, max(1, args.warmup), threads)
+    rate, kind, done, secs = cpu_reference_rate(scene, args.steps, threads, budget_s=240.0)
+    sample = f"{done} substeps of the {WORKLOAD} scene (1,048,576 particles + 262,144 diffuse pool) " \
+             f"on {threads} host threads"
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+i32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "grid": [128, 128, 128], "particles": 1048576,
+                       "diffuse_pool": 262144, "substeps_per_step": 1},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference_arm(args, ws, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from mls_mpm_b200 import DiffuseGPU, FluidGPU, scenes
+    from mls_mpm_b200.abi import check
+    scene = scenes.WORKLOADS[args.workload](seed=rank)
+    fl = FluidGPU.from_scene(scene, device=local)
+    DiffuseGPU(scene.diffuse_max).initGPU(local, fl)
+    lib, h = fl._lib, fl._scene
+    sptr = ctypes.c_void_p()
+    check(lib.mpm_get_stream(h, ctypes.byref(sptr)), "mpm_get_stream")
+    stream = torch.cuda.ExternalStream(sptr.value, device=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def launches():
+        c = ctypes.c_uint64()
+        lib.mpm_launch_count(h, ctypes.byref(c))
+        return c.value
+
+    # warm-up
+    for _ in range(args.warmup):
+        fl.simFrame()
+    fl.sync()
+    torch.cuda.synchronize()
+
+    # timed region: exactly K substeps, inputs resident in HBM
+    clocks = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    l0 = launches()
+    with clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            check(lib.mpm_step(h, 1), "mpm_step")
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        n_launch = launches() - l0
+
+        # per-phase device time over the same workload (CUDA events on the scene stream)
+        prof_steps = min(args.steps, 100)
+        lib.mpm_profile_enable(h, 1)
+        lib.mpm_profile_read(h, None, None, 1)
+        for _ in range(prof_steps):
+            check(lib.mpm_step(h, 1), "mpm_step")
+        pm = (ctypes.c_double * 10)()
+        pc = (ctypes.c_uint64 * 10)()
+        check(lib.mpm_profile_read(h, pm, pc, 1), "mpm_profile_read")
+        lib.mpm_profile_enable(h, 0)
+
+        # end to end through the public API: per step the host writes the
+        # frame's uniforms (params, walls, hand: fluid-gpu.js:295-328,
+        # 337-413, 479-527) and reads back the diffuse alive count
+        # (diffuse-gpu.js:172-188), synchronously, like the reference's frame.
+        barrier()
+        t0 = time.perf_counter()
+        for s in range(args.steps):
+            fl.updateHand([40.0, 60.0, 40.0], [0.0, 0.0, 0.0], 4.0, 1.0, False, [40.0, 60.0, 140.0])
+            fl._params_prev = None
+            fl._walls.prev_buf[:] = np.nan
+            fl.simFrame()
+            fl.diffuse.pollDebug()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+    h2d = 80 + 336 + 80
+    d2h = 4
+
+    n = scene.n
+    total_updates = n * args.steps * ws
+    value = total_updates / (ms / 1e3)
+    e2e_value = total_updates / e2e_s
+    peak, peak_src = measured_peaks()
+    G = scene.cells
+    names = [lib.mpm_phase_name(i).decode() for i in range(10)]
+    phase_ms = {names[i]: pm[i] / pc[i] for i in range(10) if pc[i]}
+    dom = max((k for k in phase_ms if k in PHASE_BYTES), key=lambda k: phase_ms[k])
+    bn, bg = PHASE_BYTES[dom]
+    dom_bytes = bn * n + bg * G
+    achieved = dom_bytes / (phase_ms[dom] * 1e-3) / 1e9
+    sub_bytes = 180 * n + 60 * G
+    sub_ms = ms / args.steps
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": phase_ms[dom]}
+    traffic = _profile_traffic(dom)
+    if traffic:
+        roofline["traffic"] = traffic
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sub_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+i32", "data": "synthetic",
+            "config": {"workload": args.workload, "grid": list(scene.grid), "particles": n,
+                       "diffuse_pool": scene.diffuse_max, "substeps_per_step": 1,
+                       "parallelism": f"scene-sharded x{ws}" if ws > 1 else "single scene",
+                       "l2": "working set > 126 MB L2 (particles 76 MB + grids 64 MB + pool 13 MB); no flush"},
+            "roofline": roofline,
+            "substep_roofline": {"achieved": sub_bytes / (sub_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                                 "frac": sub_bytes / (sub_ms * 1e-3) / 1e9 / peak,
+                                 "algorithmic_bytes": sub_bytes, "note": "180 B/particle + 60 B/cell"},
+            "phase_ms": phase_ms,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": n_launch,
+            "clocks": clocks.summary()}
+
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cpu_scene = scenes.WORKLOADS[args.workload](seed=0)
+        rate, kind, done, secs = cpu_reference_rate(cpu_scene, 40, threads, budget_s=20.0)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                                "sample": f"{done} substeps of {args.workload} ({secs:.1f} s) on {threads} threads"}
+    if dist is not None:
+        dist.barrier()
+    fl.destroy()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def _profile_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        d = json.load(open(p))
+        return d.get(WORKLOAD, {}).get(kernel)
+    except Exception:
+        return None
+
+
+if __name__ == "__main__":
+    sys.exit(main())

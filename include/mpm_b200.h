@@ -1,0 +1,198 @@
+/*
+ * mpm_b200.h — C ABI of the B200 MLS-MPM fluid + diffuse library.
+ *
+ * This is the drop-in boundary for the compute side of the reference's
+ * fluid-gpu.js (class FluidGPU) and diffuse-gpu.js (class DiffuseGPU).  A
+ * JavaScript host keeps its classes and packs the same uniform bytes it
+ * would pass to queue.writeBuffer; each entry point below replaces one
+ * WebGPU-facing member (cited as file:line).  Plain pointers and sizes only.
+ *
+ * Conventions
+ *  - Every call returns mpm_status; mpm_last_error() describes the last
+ *    failure on the calling thread.
+ *  - A scene owns one CUDA stream; calls that enqueue GPU work return without
+ *    waiting (like a WebGPU submit).  mpm_download/mpm_sync wait.
+ *  - One scene is not thread-safe; different scenes may be driven from
+ *    different threads.
+ *  - Device buffers keep the reference layouts: pos/vel vec4<f32> (16 B per
+ *    particle), affine 9 x f32 row-major, mass/density f32, cell_mv 3 x i32
+ *    per cell, cell_mass i32, cell_mv_f32 3 x f32, cell_mass_f32 f32, the
+ *    diffuse pool 48 B per slot with a u32 free list and an i32 top.
+ */
+#ifndef MPM_B200_H
+#define MPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "mpm_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_ABI_VERSION 1
+
+typedef enum mpm_status {
+    MPM_OK = 0,
+    MPM_ERR_INVALID_ARG = 1,
+    MPM_ERR_OOM = 2,
+    MPM_ERR_DEVICE = 3,
+    MPM_ERR_TIMEOUT = 4,
+    MPM_ERR_NAN = 5,
+    MPM_ERR_NO_DEVICE = 6,
+    MPM_ERR_BUSY = 7,
+    MPM_ERR_UNSUPPORTED = 8,
+    MPM_ERR_CAPACITY = 9
+} mpm_status;
+
+/* Buffers exposed by mpm_get_buffer / mpm_download / mpm_upload, named after
+ * the reference's GPUBuffer members (fluid-gpu.js:208-219, diffuse-gpu.js:52-55). */
+typedef enum mpm_buffer {
+    MPM_BUF_POS = 0,            /* particlePosBuffer     N x vec4<f32> */
+    MPM_BUF_VEL = 1,            /* particleVelBuffer     N x vec4<f32> */
+    MPM_BUF_AFFINE = 2,         /* particleAffineBuffer  N x 9 f32     */
+    MPM_BUF_MASS = 3,           /* particleMassBuffer    N x f32       */
+    MPM_BUF_DENSITY = 4,        /* particleDensityBuffer N x f32       */
+    MPM_BUF_CELL_MV = 5,        /* cellMvBuffer          G x 3 i32     */
+    MPM_BUF_CELL_MASS = 6,      /* cellMassBuffer        G x i32       */
+    MPM_BUF_CELL_MV_F32 = 7,    /* cellMvF32Buffer       G x 3 f32     */
+    MPM_BUF_CELL_MASS_F32 = 8,  /* cellMassF32Buffer     G x f32       */
+    MPM_BUF_DIFFUSE = 9,        /* DiffuseGPU.particleBuffer  M x 48 B */
+    MPM_BUF_FREE_LIST = 10,     /* DiffuseGPU.freeListBuffer  M x u32  */
+    MPM_BUF_FREE_TOP = 11       /* DiffuseGPU.freeListTopBuffer i32    */
+} mpm_buffer;
+
+/* Scene creation descriptor (FluidGPU constructor, fluid-gpu.js:10-17). */
+typedef struct mpm_desc {
+    uint32_t grid_X, grid_Y, grid_Z;  /* cells */
+    uint32_t particle_capacity;       /* particleNum: buffer capacity */
+    int32_t device;                   /* CUDA device ordinal */
+    uint32_t flags;                   /* reserved, 0 */
+} mpm_desc;
+
+typedef struct mpm_scene mpm_scene;
+
+/* ABI version (MPM_ABI_VERSION). */
+int mpm_abi_version(void);
+
+/* Text of the last error on this thread ("" if none). */
+const char* mpm_last_error(void);
+
+/* Number of visible CUDA devices (0 is not an error). */
+mpm_status mpm_device_count(int* count);
+
+/* Grid sizing of the FluidGPU constructor (fluid-gpu.js:10-16):
+ * grid_* = ceil(aspect_* / (4 * particle_radius)). */
+mpm_status mpm_desc_from_aspect(double aspect_x, double aspect_y, double aspect_z, double particle_radius,
+                                uint32_t particle_num, mpm_desc* out);
+
+/* Constructor defaults of FluidGPU (fluid-gpu.js:24-45) for this grid with
+ * dt = DT / SUBSTEPS and particle_num = 0 (fluid-gpu.js:297-313 layout). */
+mpm_status mpm_default_params(const mpm_desc* desc, mpm_params* out);
+
+/* Diffuse defaults (diffuse-gpu.js:20-31, 70-94): seed = 1. */
+mpm_status mpm_default_diffuse_params(uint32_t max_count, mpm_gen_params* gen, mpm_advect_params* adv);
+
+/* FluidGPU.initGPU -> _createBuffers (fluid-gpu.js:183-293): allocate the
+ * device buffers (zero-filled) and the scene's stream. */
+mpm_status mpm_create(const mpm_desc* desc, mpm_scene** out);
+
+/* Release every device allocation of the scene. */
+mpm_status mpm_destroy(mpm_scene* scene);
+
+/* Initial particle upload, fluid-gpu.js:278-281 (writeBuffer of pos/vel in
+ * vec4 layout, affine, mass).  Host arrays; n <= capacity becomes
+ * active_particle_num.  vel4/affine9 may be NULL (zeros). */
+mpm_status mpm_upload_particles(mpm_scene* scene, const float* pos4, const float* vel4, const float* affine9,
+                                const float* mass, uint32_t n);
+
+/* _writeParamsBuffer (fluid-gpu.js:295-328): the 80-byte Params uniform.
+ * grid dims must equal the scene's; particle_num <= capacity. */
+mpm_status mpm_set_params(mpm_scene* scene, const mpm_params* params);
+
+/* _writeWallParams upload (fluid-gpu.js:337-413): the 336-byte WallParams. */
+mpm_status mpm_set_walls(mpm_scene* scene, const mpm_wall_params* walls);
+
+/* updateHand (fluid-gpu.js:479-527): the 80-byte HandParams plus the
+ * dispatch box (_handBBoxDim*); APPLY_HAND runs iff active and all dims > 0. */
+mpm_status mpm_set_hand(mpm_scene* scene, const mpm_hand_params* hand, int active, const int32_t bbox_dims[3]);
+
+/* DiffuseGPU constructor + initGPU (diffuse-gpu.js:16-94): pool of max_count
+ * slots, free list [0..max-1], top = max, GenParams/AdvectParams uniforms.
+ * adv->diffuse_max is replaced by max_count. */
+mpm_status mpm_diffuse_enable(mpm_scene* scene, uint32_t max_count, const mpm_gen_params* gen,
+                              const mpm_advect_params* adv);
+
+/* _writeGenParams (diffuse-gpu.js:84-94): replaces the whole GenParams
+ * (thresholds and seed).  DiffuseGPU.step only rewrites the seed, so other
+ * fields changed on the host take effect only through this call. */
+mpm_status mpm_diffuse_set_gen_params(mpm_scene* scene, const mpm_gen_params* gen);
+
+/* FluidGPU.simFrame (fluid-gpu.js:648-684): runs `substeps` substeps of
+ * CLEAR..G2P (+ APPLY_HAND when active) and, when diffuse is enabled,
+ * DiffuseGPU.step (diffuse-gpu.js:148-166: seed+1, GENERATE, ADVECT) after
+ * each.  Enqueues work and returns. */
+mpm_status mpm_step(mpm_scene* scene, int substeps);
+
+/* Wait for all work enqueued on the scene's stream. */
+mpm_status mpm_sync(mpm_scene* scene);
+
+/* Device pointer and byte size of a buffer in its reference layout (valid
+ * until the next mpm_step; zero-copy hand-off to a consumer such as a
+ * renderer's vertex input, fluid-renderer.js:315-328). */
+mpm_status mpm_get_buffer(mpm_scene* scene, mpm_buffer which, void** dev_ptr, size_t* bytes);
+
+/* Copy a buffer (reference layout) to host memory; waits for the stream.
+ * `bytes` may be smaller than the buffer (a prefix is copied). */
+mpm_status mpm_download(mpm_scene* scene, mpm_buffer which, void* host_dst, size_t bytes);
+
+/* Overwrite a buffer (reference layout) from host memory (a prefix of
+ * `bytes`); used for restoring saved state. */
+mpm_status mpm_upload(mpm_scene* scene, mpm_buffer which, const void* host_src, size_t bytes);
+
+/* DiffuseGPU.requestDebugReadback + pollDebug (diffuse-gpu.js:172-188):
+ * alive = maxCount - freeListTop.  Waits for the stream. */
+mpm_status mpm_diffuse_alive_count(mpm_scene* scene, int32_t* alive);
+
+/* The scene's CUDA stream (cudaStream_t), for callers that order their own
+ * work after a step. */
+mpm_status mpm_get_stream(mpm_scene* scene, void** stream);
+
+/* ---- tracing (no counterpart in the reference, whose only timers are
+ * render-pass timestamps, fluid-renderer.js:34-41) ---- */
+
+/* Phases of a substep timed by the profiler. */
+typedef enum mpm_phase {
+    MPM_PHASE_CLEAR = 0,        /* CLEAR (shaders.js:196-210)                */
+    MPM_PHASE_P2G_MASS = 1,     /* COMPUTE_WEIGHTS + P2G_MASS (216-274)      */
+    MPM_PHASE_DECODE_MASS = 2,  /* DECODE_MASS (373-384)                     */
+    MPM_PHASE_P2G_MOM = 3,      /* P2G_MOM (276-371)                         */
+    MPM_PHASE_UPDATE_GRID = 4,  /* UPDATE_GRID (435-513)                     */
+    MPM_PHASE_APPLY_HAND = 5,   /* APPLY_HAND (394-433)                      */
+    MPM_PHASE_G2P = 6,          /* G2P (579-705)                             */
+    MPM_PHASE_DIFFUSE_GEN = 7,  /* DIFFUSE_GENERATE + slot ranking (721-856) */
+    MPM_PHASE_DIFFUSE_ADV = 8,  /* DIFFUSE_ADVECT + free-list push (858-997) */
+    MPM_PHASE_SORT = 9,         /* particle binning (no reference pass)      */
+    MPM_PHASE_COUNT = 10
+} mpm_phase;
+
+/* Name of a phase ("p2g_mom", ...), or "" for an unknown index. */
+const char* mpm_phase_name(int phase);
+
+/* Turn per-phase CUDA-event timing on the scene's stream on or off
+ * (off by default; events add a few microseconds per substep). */
+mpm_status mpm_profile_enable(mpm_scene* scene, int on);
+
+/* Accumulated per-phase GPU time (ms) and sample counts since the last
+ * reset; waits for the stream.  Arrays hold MPM_PHASE_COUNT entries. */
+mpm_status mpm_profile_read(mpm_scene* scene, double* ms, uint64_t* count, int reset);
+
+/* Number of kernels this scene has launched (CUDA kernels only). */
+mpm_status mpm_launch_count(mpm_scene* scene, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPM_B200_H */

@@ -1,0 +1,477 @@
+// mpm_capi.cu — the C ABI (include/mpm_b200.h): scene lifetime, uploads,
+// uniforms, stepping and buffer export.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm_b200.h"
+#include "mpm_kernels.h"
+#include "mpm_scene.h"
+
+static_assert(sizeof(mpm_params) == 80, "Params is 80 B (shaders.js:27-49)");
+static_assert(sizeof(mpm_wall) == 80, "Wall is 80 B (shaders.js:123-129)");
+static_assert(sizeof(mpm_wall_params) == 336, "WallParams is 16 + 4*80 B");
+static_assert(sizeof(mpm_hand_params) == 80, "HandParams is 80 B");
+static_assert(sizeof(mpm_gen_params) == 32, "GenParams is 32 B");
+static_assert(sizeof(mpm_advect_params) == 16, "AdvectParams is 16 B");
+static_assert(sizeof(mpm_diffuse_particle) == 48, "DiffuseParticle is 48 B");
+static_assert(sizeof(mpm_ray_params) == 32, "RayParams is 32 B");
+
+namespace mpm {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+
+static mpm_status fail(mpm_status st, const std::string& msg) {
+    set_error(msg);
+    return st;
+}
+
+static mpm_status cuda_fail(cudaError_t e, const char* what) {
+    const mpm_status st = (e == cudaErrorMemoryAllocation) ? MPM_ERR_OOM
+                          : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? MPM_ERR_NO_DEVICE
+                                                                                         : MPM_ERR_DEVICE;
+    return fail(st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(expr, what)                          \
+    do {                                              \
+        cudaError_t _e = (expr);                      \
+        if (_e != cudaSuccess) return cuda_fail(_e, what); \
+    } while (0)
+
+template <class T> static cudaError_t dalloc(T** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    return cudaMalloc((void**)p, bytes);
+}
+
+cudaEvent_t Scene::take_event() {
+    if (!event_pool.empty()) {
+        cudaEvent_t e = event_pool.back();
+        event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+void Scene::begin_phase(int phase, cudaEvent_t* a) {
+    (void)phase;
+    *a = nullptr;
+    if (!profile) return;
+    *a = take_event();
+    if (*a) cudaEventRecord(*a, stream);
+}
+
+void Scene::end_phase(int phase, cudaEvent_t a) {
+    if (!profile || !a) return;
+    cudaEvent_t b = take_event();
+    if (!b) { event_pool.push_back(a); return; }
+    cudaEventRecord(b, stream);
+    pending.push_back(Pending{phase, a, b});
+}
+
+cudaError_t Scene::drain_profile() {
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    for (const Pending& p : pending) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            prof_ms[p.phase] += ms;
+            prof_n[p.phase] += 1;
+        }
+        event_pool.push_back(p.a);
+        event_pool.push_back(p.b);
+    }
+    pending.clear();
+    return cudaSuccess;
+}
+
+static void free_scene(Scene& s) {
+    if (s.stream) cudaStreamSynchronize(s.stream);
+    for (const Scene::Pending& p : s.pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    for (cudaEvent_t e : s.event_pool) cudaEventDestroy(e);
+    s.pending.clear();
+    s.event_pool.clear();
+    void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
+                    s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
+                    s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.rank_state, s.diffuse.staging};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (s.diffuse.host_top) cudaFreeHost(s.diffuse.host_top);
+    if (s.stream) cudaStreamDestroy(s.stream);
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+static bool buffer_info(Scene& s, mpm_buffer which, void** ptr, size_t* bytes) {
+    const size_t N = s.capacity, G = s.G, M = s.diffuse.max_count;
+    switch (which) {
+        case MPM_BUF_POS: *ptr = s.pos; *bytes = N * 16; return true;
+        case MPM_BUF_VEL: *ptr = s.vel; *bytes = N * 16; return true;
+        case MPM_BUF_AFFINE: *ptr = s.aff; *bytes = N * 36; return true;
+        case MPM_BUF_MASS: *ptr = s.mass; *bytes = N * 4; return true;
+        case MPM_BUF_DENSITY: *ptr = s.dens; *bytes = N * 4; return true;
+        case MPM_BUF_CELL_MV: *ptr = s.mv; *bytes = G * 12; return true;
+        case MPM_BUF_CELL_MASS: *ptr = s.cm; *bytes = G * 4; return true;
+        case MPM_BUF_CELL_MV_F32: *ptr = s.mvf; *bytes = G * 12; return true;
+        case MPM_BUF_CELL_MASS_F32: *ptr = s.cmf; *bytes = G * 4; return true;
+        case MPM_BUF_DIFFUSE:
+            if (!s.diffuse.enabled) return false;
+            *ptr = s.diffuse.pool; *bytes = M * 48; return true;
+        case MPM_BUF_FREE_LIST:
+            if (!s.diffuse.enabled) return false;
+            *ptr = s.diffuse.free_list; *bytes = M * 4; return true;
+        case MPM_BUF_FREE_TOP:
+            if (!s.diffuse.enabled) return false;
+            *ptr = s.diffuse.top; *bytes = 4; return true;
+    }
+    return false;
+}
+
+}  // namespace mpm
+
+using namespace mpm;
+
+extern "C" {
+
+int mpm_abi_version(void) { return MPM_ABI_VERSION; }
+
+const char* mpm_last_error(void) { return g_err.c_str(); }
+
+mpm_status mpm_device_count(int* count) {
+    if (!count) return fail(MPM_ERR_INVALID_ARG, "count is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return MPM_OK;
+}
+
+mpm_status mpm_desc_from_aspect(double ax, double ay, double az, double r, uint32_t particle_num, mpm_desc* out) {
+    if (!out || !(r > 0.0) || !(ax > 0.0) || !(ay > 0.0) || !(az > 0.0))
+        return fail(MPM_ERR_INVALID_ARG, "aspect and radius must be positive");
+    const double normToGrid = 1.0 / (r * 4.0);   // fluid-gpu.js:11
+    std::memset(out, 0, sizeof *out);
+    out->grid_X = (uint32_t)std::ceil(ax * normToGrid);
+    out->grid_Y = (uint32_t)std::ceil(ay * normToGrid);
+    out->grid_Z = (uint32_t)std::ceil(az * normToGrid);
+    out->particle_capacity = particle_num;
+    return MPM_OK;
+}
+
+mpm_status mpm_default_params(const mpm_desc* d, mpm_params* o) {
+    if (!d || !o) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    std::memset(o, 0, sizeof *o);
+    o->grid_X = d->grid_X; o->grid_Y = d->grid_Y; o->grid_Z = d->grid_Z;
+    o->particle_num = 0;
+    o->dt = (float)(0.3 / 1.0);     // DT / SUBSTEPS (fluid-gpu.js:24,30,649)
+    o->gravity = -0.98f;
+    o->rest_density = 8.0f;
+    o->stiffness = 100.0f;
+    o->eos_power = 1.0f;
+    o->viscosity = 0.01f;
+    o->hard_min = 2.0f;             // fluid-gpu.js:41-45
+    o->hard_max_x = (float)(d->grid_X - 2);
+    o->hard_max_y = (float)(d->grid_Y - 2);
+    o->hard_max_z = (float)(d->grid_Z - 2);
+    o->wall_min = 3.0f;             // fluid-gpu.js:37-39
+    o->wall_stiffness = 1.0f;
+    o->lookahead_k = 2.0f;
+    return MPM_OK;
+}
+
+mpm_status mpm_default_diffuse_params(uint32_t max_count, mpm_gen_params* g, mpm_advect_params* a) {
+    if (!g || !a) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    g->ke_threshold = 0.5f;          // diffuse-gpu.js:20-28
+    g->spawn_rate_k = 3.0f;
+    g->density_spray_max = 1.5f;
+    g->density_bubble_min = 6.0f;
+    g->lifetime_foam = 3.0f;
+    g->pressure_threshold = 1.0f;
+    g->crest_dot_threshold = 0.3f;
+    g->seed = 1u;                    // diffuse-gpu.js:31
+    a->diffuse_max = max_count;
+    a->buoyancy = 1.2f;
+    a->drag = 4.0f;
+    a->_pad = 0.0f;
+    return MPM_OK;
+}
+
+mpm_status mpm_create(const mpm_desc* d, mpm_scene** out) {
+    if (!d || !out) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    *out = nullptr;
+    if (d->grid_X < 5 || d->grid_Y < 5 || d->grid_Z < 5)
+        return fail(MPM_ERR_INVALID_ARG, "grid must be at least 5 cells per axis");
+    const uint64_t G = (uint64_t)d->grid_X * d->grid_Y * d->grid_Z;
+    if (G >= (1ull << 31) / 3) return fail(MPM_ERR_INVALID_ARG, "grid too large for 32-bit cell indexing");
+    if (d->particle_capacity >= (1u << 31)) return fail(MPM_ERR_INVALID_ARG, "particle capacity too large");
+    int ndev = 0;
+    mpm_device_count(&ndev);
+    if (ndev == 0) return fail(MPM_ERR_NO_DEVICE, "no CUDA device");
+    if (d->device < 0 || d->device >= ndev) return fail(MPM_ERR_INVALID_ARG, "bad device ordinal");
+    DeviceGuard guard(d->device);
+    mpm_scene* sc = new (std::nothrow) mpm_scene();
+    if (!sc) return fail(MPM_ERR_OOM, "host allocation");
+    Scene& s = sc->s;
+    s.device = d->device;
+    s.X = d->grid_X; s.Y = d->grid_Y; s.Z = d->grid_Z; s.G = G;
+    s.capacity = d->particle_capacity;
+    mpm_desc dd = *d;
+    mpm_default_params(&dd, &s.params);
+    cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+    const size_t N = s.capacity;
+    if (e == cudaSuccess) e = dalloc(&s.pos, N * 16);
+    if (e == cudaSuccess) e = dalloc(&s.vel, N * 16);
+    if (e == cudaSuccess) e = dalloc(&s.aff, N * 36);
+    if (e == cudaSuccess) e = dalloc(&s.mass, N * 4);
+    if (e == cudaSuccess) e = dalloc(&s.dens, N * 4);
+    if (e == cudaSuccess) e = dalloc(&s.grid_i32, G * 16);
+    if (e == cudaSuccess) e = dalloc(&s.cmf, G * 4);
+    if (e == cudaSuccess) e = dalloc(&s.mvf, G * 12);
+    if (e != cudaSuccess) {
+        free_scene(s);
+        delete sc;
+        return cuda_fail(e, "mpm_create allocation");
+    }
+    s.cm = s.grid_i32;
+    s.mv = s.grid_i32 + G;
+    // WebGPU zero-fills new buffers (fluid-gpu.js:226-227)
+    cudaMemsetAsync(s.pos, 0, N * 16, s.stream);
+    cudaMemsetAsync(s.vel, 0, N * 16, s.stream);
+    cudaMemsetAsync(s.aff, 0, N * 36, s.stream);
+    cudaMemsetAsync(s.mass, 0, N * 4, s.stream);
+    cudaMemsetAsync(s.dens, 0, N * 4, s.stream);
+    cudaMemsetAsync(s.grid_i32, 0, G * 16, s.stream);
+    cudaMemsetAsync(s.cmf, 0, G * 4, s.stream);
+    cudaMemsetAsync(s.mvf, 0, G * 12, s.stream);
+    e = cudaStreamSynchronize(s.stream);
+    if (e != cudaSuccess) {
+        free_scene(s);
+        delete sc;
+        return cuda_fail(e, "mpm_create init");
+    }
+    *out = sc;
+    return MPM_OK;
+}
+
+mpm_status mpm_destroy(mpm_scene* sc) {
+    if (!sc) return MPM_OK;
+    DeviceGuard guard(sc->s.device);
+    if (sc->s.stream) cudaStreamSynchronize(sc->s.stream);
+    free_scene(sc->s);
+    delete sc;
+    return MPM_OK;
+}
+
+mpm_status mpm_upload_particles(mpm_scene* sc, const float* pos4, const float* vel4, const float* aff9,
+                                const float* mass, uint32_t n) {
+    if (!sc || (!pos4 && n) || (!mass && n)) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    Scene& s = sc->s;
+    if (n > s.capacity) return fail(MPM_ERR_CAPACITY, "n exceeds particle capacity");
+    DeviceGuard guard(s.device);
+    cudaStream_t st = s.stream;
+    CUDA_TRY(cudaMemcpyAsync(s.pos, pos4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "upload pos");
+    if (vel4) CUDA_TRY(cudaMemcpyAsync(s.vel, vel4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "upload vel");
+    else CUDA_TRY(cudaMemsetAsync(s.vel, 0, (size_t)n * 16, st), "zero vel");
+    if (aff9) CUDA_TRY(cudaMemcpyAsync(s.aff, aff9, (size_t)n * 36, cudaMemcpyHostToDevice, st), "upload affine");
+    else CUDA_TRY(cudaMemsetAsync(s.aff, 0, (size_t)n * 36, st), "zero affine");
+    CUDA_TRY(cudaMemcpyAsync(s.mass, mass, (size_t)n * 4, cudaMemcpyHostToDevice, st), "upload mass");
+    CUDA_TRY(cudaStreamSynchronize(st), "upload sync");
+    s.n_active = n;
+    s.params.particle_num = n;
+    return MPM_OK;
+}
+
+mpm_status mpm_set_params(mpm_scene* sc, const mpm_params* p) {
+    if (!sc || !p) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    Scene& s = sc->s;
+    if (p->grid_X != s.X || p->grid_Y != s.Y || p->grid_Z != s.Z)
+        return fail(MPM_ERR_INVALID_ARG, "params grid dims differ from the scene's");
+    if (p->particle_num > s.capacity) return fail(MPM_ERR_CAPACITY, "particle_num exceeds capacity");
+    s.params = *p;
+    s.n_active = p->particle_num;
+    return MPM_OK;
+}
+
+mpm_status mpm_set_walls(mpm_scene* sc, const mpm_wall_params* w) {
+    if (!sc || !w) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    sc->s.walls = *w;
+    return MPM_OK;
+}
+
+mpm_status mpm_set_hand(mpm_scene* sc, const mpm_hand_params* h, int active, const int32_t dims[3]) {
+    if (!sc || !h) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    Scene& s = sc->s;
+    s.hand = *h;
+    s.hand_active = active ? 1 : 0;
+    for (int i = 0; i < 3; ++i) s.hand_dims[i] = dims ? dims[i] : 0;
+    return MPM_OK;
+}
+
+mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_params* gen,
+                              const mpm_advect_params* adv) {
+    if (!sc || !gen || !adv) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    if (max_count == 0 || max_count >= (1u << 30)) return fail(MPM_ERR_INVALID_ARG, "bad diffuse max_count");
+    Scene& s = sc->s;
+    DeviceGuard guard(s.device);
+    DiffuseState& d = s.diffuse;
+    if (d.enabled) return fail(MPM_ERR_BUSY, "diffuse already enabled");
+    const size_t M = max_count, N = s.capacity;
+    const size_t nwN = (N + 31) / 32, nwM = (M + 31) / 32;
+    const size_t nb = std::max((nwN + kRankThreads - 1) / kRankThreads, (nwM + kRankThreads - 1) / kRankThreads) + 1;
+    cudaError_t e = dalloc(&d.pool, M * 48);
+    if (e == cudaSuccess) e = dalloc(&d.free_list, M * 4);
+    if (e == cudaSuccess) e = dalloc(&d.top, 16);
+    if (e == cudaSuccess) e = dalloc(&d.spawn_bits, nwN * 4);
+    if (e == cudaSuccess) e = dalloc(&d.kill_bits, nwM * 4);
+    if (e == cudaSuccess) e = dalloc(&d.block_counts, nb * 4);
+    if (e == cudaSuccess) e = dalloc(&d.rank_state, 16);
+    if (e == cudaSuccess) e = dalloc(&d.staging, N * 48);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&d.host_top, 16);
+    if (e != cudaSuccess) return cuda_fail(e, "mpm_diffuse_enable allocation");
+    // diffuse-gpu.js:60-68: free list [0..M-1], top = M, all slots dead
+    std::vector<uint32_t> fl(M);
+    for (size_t i = 0; i < M; ++i) fl[i] = (uint32_t)i;
+    const int32_t top = (int32_t)M;
+    CUDA_TRY(cudaMemcpyAsync(d.free_list, fl.data(), M * 4, cudaMemcpyHostToDevice, s.stream), "free list");
+    CUDA_TRY(cudaMemcpyAsync(d.top, &top, 4, cudaMemcpyHostToDevice, s.stream), "top");
+    CUDA_TRY(cudaMemsetAsync(d.pool, 0, M * 48, s.stream), "pool");
+    CUDA_TRY(cudaStreamSynchronize(s.stream), "diffuse init sync");
+    d.max_count = (uint32_t)M;
+    d.gen = *gen;
+    d.adv = *adv;
+    d.adv.diffuse_max = (uint32_t)M;
+    d.seed = gen->seed;
+    d.enabled = true;
+    return MPM_OK;
+}
+
+mpm_status mpm_diffuse_set_gen_params(mpm_scene* sc, const mpm_gen_params* gen) {
+    if (!sc || !gen) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    if (!sc->s.diffuse.enabled) return fail(MPM_ERR_INVALID_ARG, "diffuse not enabled");
+    sc->s.diffuse.gen = *gen;
+    sc->s.diffuse.seed = gen->seed;
+    return MPM_OK;
+}
+
+mpm_status mpm_step(mpm_scene* sc, int substeps) {
+    if (!sc || substeps < 0) return fail(MPM_ERR_INVALID_ARG, "bad argument");
+    Scene& s = sc->s;
+    DeviceGuard guard(s.device);
+    for (int i = 0; i < substeps; ++i) {
+        cudaError_t e = launch_substep(s);
+        if (e != cudaSuccess) return cuda_fail(e, "mpm_step launch");
+    }
+    return MPM_OK;
+}
+
+mpm_status mpm_sync(mpm_scene* sc) {
+    if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    DeviceGuard guard(sc->s.device);
+    CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "mpm_sync");
+    return MPM_OK;
+}
+
+mpm_status mpm_get_buffer(mpm_scene* sc, mpm_buffer which, void** dev_ptr, size_t* bytes) {
+    if (!sc || !dev_ptr || !bytes) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    if (!buffer_info(sc->s, which, dev_ptr, bytes)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
+    return MPM_OK;
+}
+
+mpm_status mpm_download(mpm_scene* sc, mpm_buffer which, void* host_dst, size_t bytes) {
+    if (!sc || (!host_dst && bytes)) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    void* p;
+    size_t sz;
+    if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
+    if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
+    DeviceGuard guard(sc->s.device);
+    CUDA_TRY(cudaMemcpyAsync(host_dst, p, bytes, cudaMemcpyDeviceToHost, sc->s.stream), "download");
+    CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "download sync");
+    return MPM_OK;
+}
+
+mpm_status mpm_upload(mpm_scene* sc, mpm_buffer which, const void* host_src, size_t bytes) {
+    if (!sc || (!host_src && bytes)) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    void* p;
+    size_t sz;
+    if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
+    if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
+    DeviceGuard guard(sc->s.device);
+    CUDA_TRY(cudaMemcpyAsync(p, host_src, bytes, cudaMemcpyHostToDevice, sc->s.stream), "upload");
+    CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "upload sync");
+    return MPM_OK;
+}
+
+mpm_status mpm_diffuse_alive_count(mpm_scene* sc, int32_t* alive) {
+    if (!sc || !alive) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    DiffuseState& d = sc->s.diffuse;
+    if (!d.enabled) return fail(MPM_ERR_INVALID_ARG, "diffuse not enabled");
+    DeviceGuard guard(sc->s.device);
+    CUDA_TRY(cudaMemcpyAsync(d.host_top, d.top, 4, cudaMemcpyDeviceToHost, sc->s.stream), "top readback");
+    CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "top sync");
+    *alive = (int32_t)d.max_count - *d.host_top;
+    return MPM_OK;
+}
+
+mpm_status mpm_get_stream(mpm_scene* sc, void** stream) {
+    if (!sc || !stream) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    *stream = (void*)sc->s.stream;
+    return MPM_OK;
+}
+
+static const char* const kPhaseNames[MPM_PHASE_COUNT] = {
+    "clear", "p2g_mass", "decode_mass", "p2g_mom", "update_grid", "apply_hand", "g2p",
+    "diffuse_generate", "diffuse_advect", "sort"};
+
+const char* mpm_phase_name(int phase) {
+    if (phase < 0 || phase >= MPM_PHASE_COUNT) return "";
+    return kPhaseNames[phase];
+}
+
+mpm_status mpm_profile_enable(mpm_scene* sc, int on) {
+    if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    sc->s.profile = on != 0;
+    return MPM_OK;
+}
+
+mpm_status mpm_profile_read(mpm_scene* sc, double* ms, uint64_t* count, int reset) {
+    if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    Scene& s = sc->s;
+    DeviceGuard guard(s.device);
+    CUDA_TRY(s.drain_profile(), "mpm_profile_read");
+    for (int i = 0; i < MPM_PHASE_COUNT; ++i) {
+        if (ms) ms[i] = s.prof_ms[i];
+        if (count) count[i] = s.prof_n[i];
+        if (reset) { s.prof_ms[i] = 0.0; s.prof_n[i] = 0; }
+    }
+    return MPM_OK;
+}
+
+mpm_status mpm_launch_count(mpm_scene* sc, uint64_t* launches) {
+    if (!sc || !launches) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    *launches = sc->s.launches;
+    return MPM_OK;
+}
+
+}  // extern "C"

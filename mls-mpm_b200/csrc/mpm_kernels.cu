@@ -1,0 +1,763 @@
+// mpm_kernels.cu — per-pass CUDA kernels of the MLS-MPM substep and the
+// diffuse spray/foam update, one kernel per reference compute shader.
+//
+// Compiled with --fmad=false; see mpm_device.cuh for the numerics contract.
+// Each kernel restates the WGSL shader named in its comment with the same
+// loop order and operation order, so per-particle f32 results and i32 grid
+// contributions are bit-identical to the reference's.  Grid accumulation uses
+// 32-bit integer atomics, whose sum does not depend on the order of arrival.
+//
+// Memory safety: the reference leaves P2G_MOM's and G2P's stencil indices
+// unchecked (shaders.js:303-304, 598-599) and relies on particles staying in
+// [2, dim-2].  Here a linear stencil index outside the grid buffer is skipped
+// (reads give 0, writes are dropped), which changes nothing for particles that
+// keep the reference's invariant and never touches memory outside the buffer.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mpm_device.cuh"
+#include "mpm_kernels.h"
+
+namespace mpm {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// P2G_MASS (shaders.js:242-274), weights of COMPUTE_WEIGHTS (shaders.js:216-240)
+// recomputed in registers.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_p2g_mass(const float4* __restrict__ pos, const float* __restrict__ mass,
+                                                        int32_t* __restrict__ cm, uint32_t n, int32_t X, int32_t Y,
+                                                        int32_t Z) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const float4 q = pos[p];
+    const float pm = mass[p];
+    int32_t cx, cy, cz;
+    float fx, fy, fz;
+    cell_frac(q.x, cx, fx);
+    cell_frac(q.y, cy, fy);
+    cell_frac(q.z, cz, fz);
+    float wx[3], wy[3], wz[3];
+    qweights(fx, wx[0], wx[1], wx[2]);
+    qweights(fy, wy[0], wy[1], wy[2]);
+    qweights(fz, wz[0], wz[1], wz[2]);
+    const int32_t bx = cx - 1, by = cy - 1, bz = cz - 1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int32_t zz = bz + k;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int32_t yy = by + j;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int32_t xx = bx + i;
+                if (xx < 0 || xx >= X || yy < 0 || yy >= Y || zz < 0 || zz >= Z) continue;
+                const int32_t idx = (zz * Y + yy) * X + xx;
+                const float w = wx[i] * wy[j] * wz[k];
+                atomicAdd(&cm[idx], encode(w * pm));
+            }
+        }
+    }
+}
+
+// DECODE_MASS (shaders.js:373-384)
+__global__ void __launch_bounds__(kThreads) k_decode_mass(const int32_t* __restrict__ cm, float* __restrict__ cmf,
+                                                           uint64_t G) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < G) cmf[i] = decode(cm[i]);
+}
+
+// ---------------------------------------------------------------------------
+// P2G_MOM (shaders.js:276-371)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_p2g_mom(const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                       const float* __restrict__ aff, const float* __restrict__ mass,
+                                                       const float* __restrict__ cmf, int32_t* __restrict__ mv,
+                                                       float* __restrict__ dens, const mpm_params P, uint32_t G) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.particle_num) return;
+    const float4 q = pos[p];
+    const float4 v = vel[p];
+    const float m = mass[p];
+    const float* a = aff + 9ull * p;
+    const float a00 = a[0], a01 = a[1], a02 = a[2], a10 = a[3], a11 = a[4], a12 = a[5], a20 = a[6], a21 = a[7],
+                a22 = a[8];
+    int32_t cx, cy, cz;
+    float fx, fy, fz;
+    cell_frac(q.x, cx, fx);
+    cell_frac(q.y, cy, fy);
+    cell_frac(q.z, cz, fz);
+    float wx[3], wy[3], wz[3];
+    qweights(fx, wx[0], wx[1], wx[2]);
+    qweights(fy, wy[0], wy[1], wy[2]);
+    qweights(fz, wz[0], wz[1], wz[2]);
+    const uint32_t X = P.grid_X, Y = P.grid_Y;
+    const uint32_t SLICE = X * Y;
+    const uint32_t baseIdx = (uint32_t)(((cz - 1) * (int32_t)Y + (cy - 1)) * (int32_t)X + (cx - 1));
+
+    float density = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
+                const float cmass = cidx < G ? cmf[cidx] : 0.0f;
+                density += wx[i] * wy[j] * wz[k] * cmass;
+            }
+    dens[p] = density;
+    if (density <= 1e-8f) return;
+
+    const float rest = P.rest_density;
+    const float vol = __fdiv_rn(m, fmaxf(density, rest * 0.15f));
+    float pressure = P.stiffness * (eos_pow(__fdiv_rn(density, rest), P.eos_power) - 1.0f);
+    const float pFloor = density > rest * kCohesionGate ? kCohesionPressure : 0.0f;
+    pressure = fmaxf(pressure, pFloor);
+    const float visc = P.viscosity;
+    const float s00 = -pressure + visc * (a00 + a00);
+    const float s11 = -pressure + visc * (a11 + a11);
+    const float s22 = -pressure + visc * (a22 + a22);
+    const float s01 = visc * (a01 + a10);
+    const float s02 = visc * (a02 + a20);
+    const float s12 = visc * (a12 + a21);
+    const float coef = -vol * 4.0f * P.dt;
+    const float dxs[3] = {-fx - 1.0f, -fx, 1.0f - fx};
+    const float dys[3] = {-fy - 1.0f, -fy, 1.0f - fy};
+    const float dzs[3] = {-fz - 1.0f, -fz, 1.0f - fz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float wzk = wz[k], dzk = dzs[k];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float wyzk = wy[j] * wzk, dyj = dys[j];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float w = wx[i] * wyzk;
+                const float dxi = dxs[i];
+                const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
+                const float Qx = a00 * dxi + a01 * dyj + a02 * dzk;
+                const float Qy = a10 * dxi + a11 * dyj + a12 * dzk;
+                const float Qz = a20 * dxi + a21 * dyj + a22 * dzk;
+                const float fxf = coef * (s00 * dxi + s01 * dyj + s02 * dzk);
+                const float fyf = coef * (s01 * dxi + s11 * dyj + s12 * dzk);
+                const float fzf = coef * (s02 * dxi + s12 * dyj + s22 * dzk);
+                if (cidx < G) {
+                    int32_t* c = mv + 3ull * cidx;
+                    atomicAdd(c + 0, encode(w * (m * (v.x + Qx) + fxf)));
+                    atomicAdd(c + 1, encode(w * (m * (v.y + Qy) + fyf)));
+                    atomicAdd(c + 2, encode(w * (m * (v.z + Qz) + fzf)));
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// UPDATE_GRID (shaders.js:435-513)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_update_grid(const int32_t* __restrict__ mv,
+                                                           const int32_t* __restrict__ cm, float* __restrict__ mvf,
+                                                           const mpm_params P, const mpm_wall_params W) {
+    const uint32_t X = P.grid_X, Y = P.grid_Y, Z = P.grid_Z;
+    const uint64_t G = (uint64_t)X * Y * Z;
+    const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= G) return;
+    const float c = decode(cm[idx]);
+    float* out = mvf + 3 * idx;
+    if (c <= 0.0f) { out[0] = 0.0f; out[1] = 0.0f; out[2] = 0.0f; return; }
+    float vx = __fdiv_rn(decode(mv[3 * idx + 0]), c);
+    float vy = __fdiv_rn(decode(mv[3 * idx + 1]), c);
+    float vz = __fdiv_rn(decode(mv[3 * idx + 2]), c);
+    vy += P.gravity * P.dt;
+    const int32_t cx = (int32_t)(idx % X);
+    const int32_t cy = (int32_t)((idx / X) % Y);
+    const int32_t cz = (int32_t)(idx / ((uint64_t)X * Y));
+    if (cx < 2 || cx > (int32_t)X - 3) vx = 0.0f;
+    if (cy < 2 && vy < 0.0f) vy = 0.0f;
+    if (cy > (int32_t)Y - 3 && vy > 0.0f) vy = 0.0f;
+    if (cz < 2 || cz > (int32_t)Z - 3) vz = 0.0f;
+    if (cy < 2) { vx *= 0.85f; vz *= 0.9f; }
+    const uint32_t nw = wall_count_of(W.count_pad[0]);
+    if (nw > 0) {
+        const f3 cellPos = mk(__int2float_rn(cx) + 0.5f, __int2float_rn(cy) + 0.5f, __int2float_rn(cz) + 0.5f);
+        f3 wv = mk(vx, vy, vz);
+        for (uint32_t wi = 0; wi < nw; ++wi) {
+            const WallD w = load_wall(W.walls[wi]);
+            const f3 lp = wall_to_local(cellPos, w);
+            if (lp.x < w.mn.x - 1.0f || lp.y < w.mn.y - 1.0f || lp.z < w.mn.z - 1.0f || lp.x > w.mx.x + 1.0f ||
+                lp.y > w.mx.y + 1.0f || lp.z > w.mx.z + 1.0f)
+                continue;
+            const f3 wvel = wall_vel_at(cellPos, w);
+            f3 n;
+            const float sw = wall_sdf_normal(lp, w.mn, w.mx, n);
+            if (sw < 0.0f) {
+                wv = wvel;
+            } else if (sw < 1.0f) {
+                const f3 nn = wall_to_world_dir(n, w);
+                const f3 vrel = sub(wv, wvel);
+                const float vn = dot3(vrel, nn);
+                if (vn < 0.0f) wv = mk(wv.x - vn * nn.x, wv.y - vn * nn.y, wv.z - vn * nn.z);
+            }
+        }
+        vx = wv.x; vy = wv.y; vz = wv.z;
+    }
+    out[0] = vx; out[1] = vy; out[2] = vz;
+}
+
+// ---------------------------------------------------------------------------
+// APPLY_HAND (shaders.js:394-433): 4x4x4 groups over the CPU-computed box.
+// ---------------------------------------------------------------------------
+__global__ void k_apply_hand(float* __restrict__ mvf, const mpm_params P, const mpm_hand_params H) {
+    if (H.is_on == 0u) return;
+    const int32_t cx = H.bbox_min_x + (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int32_t cy = H.bbox_min_y + (int32_t)(blockIdx.y * blockDim.y + threadIdx.y);
+    const int32_t cz = H.bbox_min_z + (int32_t)(blockIdx.z * blockDim.z + threadIdx.z);
+    if (cx > H.bbox_max_x || cy > H.bbox_max_y || cz > H.bbox_max_z) return;
+    if (cx < 0 || cy < 0 || cz < 0 || cx >= (int32_t)P.grid_X || cy >= (int32_t)P.grid_Y || cz >= (int32_t)P.grid_Z)
+        return;
+    const uint32_t idx = (uint32_t)((cz * (int32_t)P.grid_Y + cy) * (int32_t)P.grid_X + cx);
+    const f3 cell = mk(__int2float_rn(cx) + 0.5f, __int2float_rn(cy) + 0.5f, __int2float_rn(cz) + 0.5f);
+    const f3 hp = mk(H.px, H.py, H.pz);
+    const f3 dv = sub(hp, mk(H.ex, H.ey, H.ez));
+    const float dl = len3(dv);
+    const f3 dir = mk(__fdiv_rn(dv.x, dl), __fdiv_rn(dv.y, dl), __fdiv_rn(dv.z, dl));
+    const f3 to_cell = sub(cell, hp);
+    const float t0 = dot3(to_cell, dir);
+    const f3 perp = mk(to_cell.x - t0 * dir.x, to_cell.y - t0 * dir.y, to_cell.z - t0 * dir.z);
+    const float d = len3(perp);
+    if (d >= H.radius) return;
+    const float t = 1.0f - __fdiv_rn(d, H.radius);
+    const float w = t * t * H.strength;
+    mvf[idx * 3u + 0u] += H.vx * w;
+    mvf[idx * 3u + 1u] += H.vy * w;
+    mvf[idx * 3u + 2u] += H.vz * w;
+}
+
+// ---------------------------------------------------------------------------
+// G2P (shaders.js:579-705)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_g2p(float4* __restrict__ pos, float4* __restrict__ vel,
+                                                   float* __restrict__ aff, const float* __restrict__ mvf,
+                                                   const mpm_params P, const mpm_wall_params W, uint32_t G) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.particle_num) return;
+    const float4 q = pos[p];
+    int32_t cx, cy, cz;
+    float fx, fy, fz;
+    cell_frac(q.x, cx, fx);
+    cell_frac(q.y, cy, fy);
+    cell_frac(q.z, cz, fz);
+    float wx[3], wy[3], wz[3];
+    qweights(fx, wx[0], wx[1], wx[2]);
+    qweights(fy, wy[0], wy[1], wy[2]);
+    qweights(fz, wz[0], wz[1], wz[2]);
+    const int32_t bx = cx - 1, by = cy - 1, bz = cz - 1;
+    const uint32_t X = P.grid_X, Y = P.grid_Y;
+    const uint32_t SLICE = X * Y;
+    const uint32_t baseIdx = (uint32_t)((bz * (int32_t)Y + by) * (int32_t)X + bx);
+    float gvx = 0.0f, gvy = 0.0f, gvz = 0.0f;
+    float B00 = 0.0f, B01 = 0.0f, B02 = 0.0f, B10 = 0.0f, B11 = 0.0f, B12 = 0.0f, B20 = 0.0f, B21 = 0.0f, B22 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float wzk = wz[k];
+        const float dzk = __int2float_rn(bz + k) - q.z + 0.5f;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float wyzk = wy[j] * wzk;
+            const float dyj = __int2float_rn(by + j) - q.y + 0.5f;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float w = wx[i] * wyzk;
+                const float dxi = __int2float_rn(bx + i) - q.x + 0.5f;
+                const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
+                float cvx = 0.0f, cvy = 0.0f, cvz = 0.0f;
+                if (cidx < G) {
+                    const float* c = mvf + 3ull * cidx;
+                    cvx = c[0]; cvy = c[1]; cvz = c[2];
+                }
+                const float wvx = w * cvx, wvy = w * cvy, wvz = w * cvz;
+                gvx += wvx; gvy += wvy; gvz += wvz;
+                B00 += wvx * dxi; B01 += wvx * dyj; B02 += wvx * dzk;
+                B10 += wvy * dxi; B11 += wvy * dyj; B12 += wvy * dzk;
+                B20 += wvz * dxi; B21 += wvz * dyj; B22 += wvz * dzk;
+            }
+        }
+    }
+    float* a = aff + 9ull * p;
+    a[0] = B00 * 4.0f; a[1] = B01 * 4.0f; a[2] = B02 * 4.0f;
+    a[3] = B10 * 4.0f; a[4] = B11 * 4.0f; a[5] = B12 * 4.0f;
+    a[6] = B20 * 4.0f; a[7] = B21 * 4.0f; a[8] = B22 * 4.0f;
+
+    const float dt = P.dt, lk = P.lookahead_k, ws = P.wall_stiffness;
+    f3 np = mk(q.x + dt * gvx, q.y + dt * gvy, q.z + dt * gvz);
+    f3 nv = mk(gvx, gvy, gvz);
+    const float floorZoneY = P.hard_min + kFloorBand;
+    const float xny = np.y + nv.y * dt * lk;
+    if (xny < floorZoneY) {
+        const float distBelowFloor = floorZoneY - xny;
+        const float blend = wclamp(__fdiv_rn(distBelowFloor, kFloorBand), 0.0f, 1.0f);
+        nv.y += ws * blend * distBelowFloor;
+    }
+    const uint32_t nw = wall_count_of(W.count_pad[0]);
+    for (uint32_t wi = 0; wi < nw; ++wi) {
+        const WallD w = load_wall(W.walls[wi]);
+        const f3 xnw = mk(np.x + nv.x * dt * lk, np.y + nv.y * dt * lk, np.z + nv.z * dt * lk);
+        const f3 lxn = wall_to_local(xnw, w);
+        if (inside_open(lxn, w.mn, w.mx)) {
+            f3 nl;
+            const float sw = wall_sdf_normal(lxn, w.mn, w.mx, nl);
+            const float dist = -sw;
+            const float blend = wclamp(__fdiv_rn(dist, P.wall_min), 0.0f, 1.0f);
+            const f3 nwd = wall_to_world_dir(nl, w);
+            const float sc = ws * blend * dist;
+            nv = mk(nv.x + nwd.x * sc, nv.y + nwd.y * sc, nv.z + nwd.z * sc);
+        }
+        const f3 lnp = wall_to_local(np, w);
+        if (inside_open(lnp, w.mn, w.mx)) {
+            f3 nl;
+            const float sw = wall_sdf_normal(lnp, w.mn, w.mx, nl);
+            const f3 nn = wall_to_world_dir(nl, w);
+            const float mm = fmaxf(sw, -0.5f);
+            np = mk(np.x - nn.x * mm, np.y - nn.y * mm, np.z - nn.z * mm);
+            const float vn = dot3(sub(nv, wall_vel_at(np, w)), nn);
+            if (vn < 0.0f) nv = mk(nv.x - vn * nn.x, nv.y - vn * nn.y, nv.z - vn * nn.z);
+        }
+    }
+    const float hmin = P.hard_min;
+    if (np.x < hmin) { np.x = hmin; nv.x = 0.0f; }
+    if (np.x > P.hard_max_x) { np.x = P.hard_max_x; nv.x = 0.0f; }
+    if (np.y < hmin) { np.y = hmin; nv.y = 0.0f; }
+    if (np.y > P.hard_max_y) { np.y = P.hard_max_y; nv.y = 0.0f; }
+    if (np.z < hmin) { np.z = hmin; nv.z = 0.0f; }
+    if (np.z > P.hard_max_z) { np.z = P.hard_max_z; nv.z = 0.0f; }
+    pos[p] = make_float4(np.x, np.y, np.z, 0.0f);
+    vel[p] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Diffuse GENERATE (shaders.js:721-856), split in three so that slot
+// assignment is deterministic: (1) every particle decides whether it spawns
+// and stages its record at staging[id], setting bit id; (2) popcounts + one
+// scan give each spawner its rank among spawners in ascending id; (3) the
+// spawner of rank r takes free_list[top-1-r] if r < top — exactly the slots a
+// one-at-a-time try_spawn (shaders.js:791-798) hands out in ascending id.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool estimate_normal(const float* __restrict__ cmf, const mpm_params& P, float px,
+                                                float py, float pz, f3& n) {
+    const int32_t X = P.grid_X, Y = P.grid_Y, Z = P.grid_Z;
+    const int32_t gx = __float2int_rz(floorf(px)), gy = __float2int_rz(floorf(py)), gz = __float2int_rz(floorf(pz));
+    if (gx < 1 || gx >= X - 1 || gy < 1 || gy >= Y - 1 || gz < 1 || gz >= Z - 1) return false;
+    const uint32_t idxL = (uint32_t)((gz * Y + gy) * X + (gx - 1));
+    const uint32_t idxR = (uint32_t)((gz * Y + gy) * X + (gx + 1));
+    const uint32_t idxD = (uint32_t)((gz * Y + (gy - 1)) * X + gx);
+    const uint32_t idxU = (uint32_t)((gz * Y + (gy + 1)) * X + gx);
+    const uint32_t idxB = (uint32_t)(((gz - 1) * Y + gy) * X + gx);
+    const uint32_t idxF = (uint32_t)(((gz + 1) * Y + gy) * X + gx);
+    const f3 v = mk(cmf[idxL] - cmf[idxR], cmf[idxD] - cmf[idxU], cmf[idxB] - cmf[idxF]);
+    const float len = len3(v);
+    if (len < 1e-6f) return false;
+    n = mk(__fdiv_rn(v.x, len), __fdiv_rn(v.y, len), __fdiv_rn(v.z, len));
+    return true;
+}
+
+// Spawn decision + record for fluid particle `id` with post-G2P pos/vel.
+__device__ __forceinline__ bool diffuse_spawn_record(uint32_t id, float4 q, float4 v, float m, float density,
+                                                     const float* __restrict__ cmf, const mpm_params& P,
+                                                     const mpm_gen_params& gen, mpm_diffuse_particle& r) {
+    if (density <= 0.0f || density > gen.density_bubble_min) return false;
+    const f3 vel = mk(v.x, v.y, v.z);
+    const float speed2 = dot3(vel, vel);
+    const float speed = __fsqrt_rn(speed2);
+    const float ke = 0.5f * m * speed2;
+    const float rest = P.rest_density;
+    float pressure = P.stiffness * (eos_pow(__fdiv_rn(density, rest), P.eos_power) - 1.0f);
+    const float pFloor = density > rest * kCohesionGate ? kCohesionPressure : 0.0f;
+    pressure = fmaxf(pressure, pFloor);
+    const float trappedAir = fmaxf(0.0f, pressure - gen.pressure_threshold);
+    f3 nrm;
+    const bool ok = estimate_normal(cmf, P, q.x, q.y, q.z, nrm);
+    float waveCrest = 0.0f;
+    if (speed > 1e-4f && ok) {
+        const f3 vs = mk(__fdiv_rn(vel.x, speed), __fdiv_rn(vel.y, speed), __fdiv_rn(vel.z, speed));
+        const float dotVal = dot3(vs, nrm);
+        if (dotVal > gen.crest_dot_threshold) waveCrest = dotVal * speed;
+    }
+    const float score = ke + trappedAir * 2.0f + waveCrest * 1.5f;
+    if (score < gen.ke_threshold) return false;
+    const uint32_t randSeed = id * 9781u + gen.seed;
+    const float spawnChance = fminf(1.0f, (score - gen.ke_threshold) * gen.spawn_rate_k * P.dt);
+    if (diffuse_rand(randSeed) > spawnChance) return false;
+    const float jitter = 0.3f;
+    const float jx = (diffuse_rand(randSeed + 1u) - 0.5f) * jitter * speed;
+    const float jy = (diffuse_rand(randSeed + 2u) - 0.5f) * jitter * speed;
+    const float jz = (diffuse_rand(randSeed + 3u) - 0.5f) * jitter * speed;
+    uint32_t ptype = MPM_DIFFUSE_FOAM;
+    if (density < gen.density_spray_max) ptype = MPM_DIFFUSE_SPRAY;
+    const float lifetime =
+        ptype == MPM_DIFFUSE_FOAM ? gen.lifetime_foam * fminf(1.0f, __fdiv_rn(score, gen.ke_threshold)) : 999.0f;
+    r.pos[0] = q.x; r.pos[1] = q.y; r.pos[2] = q.z; r.pos[3] = 0.0f;
+    r.vel[0] = vel.x + jx; r.vel[1] = vel.y + jy; r.vel[2] = vel.z + jz; r.vel[3] = 0.0f;
+    r.ptype = ptype; r.alive = 1u; r.lifetime = lifetime; r._pad = 0.0f;
+    return true;
+}
+
+__global__ void __launch_bounds__(kThreads) k_diffuse_gen_eval(const float4* __restrict__ pos,
+                                                                const float4* __restrict__ vel,
+                                                                const float* __restrict__ mass,
+                                                                const float* __restrict__ dens,
+                                                                const float* __restrict__ cmf, const mpm_params P,
+                                                                const mpm_gen_params gen,
+                                                                mpm_diffuse_particle* __restrict__ staging,
+                                                                uint32_t* __restrict__ bits) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    bool s = false;
+    if (p < P.particle_num) {
+        mpm_diffuse_particle r;
+        s = diffuse_spawn_record(p, pos[p], vel[p], mass[p], dens[p], cmf, P, gen, r);
+        if (s) staging[p] = r;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, s);
+    if ((threadIdx.x & 31) == 0 && (p >> 5) < (P.particle_num + 31u) / 32u) bits[p >> 5] = b;
+}
+
+// popcount of each kRankThreads-word group of a bitmask.
+__global__ void __launch_bounds__(kRankThreads) k_bits_count(const uint32_t* __restrict__ bits, uint32_t nwords,
+                                                              uint32_t* __restrict__ counts) {
+    const uint32_t w = blockIdx.x * kRankThreads + threadIdx.x;
+    uint32_t c = w < nwords ? __popc(bits[w]) : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    __shared__ uint32_t ws[kRankThreads / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int i = 0; i < kRankThreads / 32; ++i) t += ws[i];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the group counts (one block).  Applies the pass to the
+// free-list top: mode 0 (spawn) pops min(total, top) slots when top > 0,
+// mode 1 (kill) pushes total slots.  state = {top before, total, applied}.
+__global__ void __launch_bounds__(1024) k_rank_scan(uint32_t* __restrict__ counts, uint32_t nb,
+                                                     int32_t* __restrict__ top, int32_t* __restrict__ state,
+                                                     int mode) {
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < nb ? counts[i] : 0u;
+        uint32_t x = v;
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) ws[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t s = ws[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            ws[lane] = s;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + (wid > 0 ? ws[wid - 1] : 0u) + x - v;
+        if (i < nb) counts[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += ws[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const int32_t t0 = *top;
+        const int32_t total = (int32_t)carry;
+        int32_t applied;
+        if (mode == 0) {
+            applied = t0 > 0 ? (total < t0 ? total : t0) : 0;
+            *top = t0 - applied;
+        } else {
+            applied = total;
+            *top = t0 + total;
+        }
+        state[0] = t0; state[1] = total; state[2] = applied;
+    }
+}
+
+// Rank of each set bit: group offset + exclusive popcount within the group.
+__device__ __forceinline__ uint32_t group_rank_base(uint32_t word, const uint32_t* __restrict__ counts) {
+    __shared__ uint32_t ws[kRankThreads / 32];
+    const uint32_t c = __popc(word);
+    uint32_t x = c;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[wid] = x;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int i = 0; i < wid; ++i) before += ws[i];
+    return counts[blockIdx.x] + before + x - c;
+}
+
+__global__ void __launch_bounds__(kRankThreads) k_diffuse_gen_write(const uint32_t* __restrict__ bits,
+                                                                     uint32_t nwords,
+                                                                     const uint32_t* __restrict__ counts,
+                                                                     const int32_t* __restrict__ state,
+                                                                     const uint32_t* __restrict__ free_list,
+                                                                     const mpm_diffuse_particle* __restrict__ staging,
+                                                                     mpm_diffuse_particle* __restrict__ pool) {
+    const uint32_t w = blockIdx.x * kRankThreads + threadIdx.x;
+    uint32_t word = w < nwords ? bits[w] : 0u;
+    uint32_t r = group_rank_base(word, counts);
+    const int32_t t0 = state[0], applied = state[2];
+    while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        if ((int32_t)r < applied) {
+            const uint32_t slot = free_list[(uint32_t)(t0 - 1 - (int32_t)r)];
+            pool[slot] = staging[w * 32u + (uint32_t)b];
+        }
+        ++r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Diffuse ADVECT (shaders.js:858-997).  Kills set alive = 0 and a bit per
+// slot; k_diffuse_kill_push then pushes killed slots in ascending slot order
+// (the order a one-at-a-time kill_particle, shaders.js:914-918, produces).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ f3 sample_grid_velocity(const float* __restrict__ mvf, const mpm_params& P, f3 pos) {
+    const int32_t X = P.grid_X, Y = P.grid_Y, Z = P.grid_Z;
+    int32_t cx, cy, cz;
+    float fx, fy, fz;
+    cell_frac(pos.x, cx, fx);
+    cell_frac(pos.y, cy, fy);
+    cell_frac(pos.z, cz, fz);
+    float wx[3], wy[3], wz[3];
+    qweights(fx, wx[0], wx[1], wx[2]);
+    qweights(fy, wy[0], wy[1], wy[2]);
+    qweights(fz, wz[0], wz[1], wz[2]);
+    f3 v = mk(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int32_t zz = cz - 1 + k;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int32_t yy = cy - 1 + j;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int32_t xx = cx - 1 + i;
+                if (xx < 0 || xx >= X || yy < 0 || yy >= Y || zz < 0 || zz >= Z) continue;
+                const uint32_t idx = (uint32_t)((zz * Y + yy) * X + xx);
+                const float w = wx[i] * wy[j] * wz[k];
+                v.x += w * mvf[idx * 3u + 0u];
+                v.y += w * mvf[idx * 3u + 1u];
+                v.z += w * mvf[idx * 3u + 2u];
+            }
+        }
+    }
+    return v;
+}
+
+__device__ __forceinline__ void reflect_axis(float& p, float& v, float lo, float hi) {
+    float np = p, nv = v;
+    if (np < lo) { np = lo + (lo - np); nv = -nv * kRestitution; }
+    else if (np > hi) { np = hi - (np - hi); nv = -nv * kRestitution; }
+    p = wclamp(np, lo, hi);
+    v = nv;
+}
+
+__global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particle* __restrict__ pool,
+                                                              const float* __restrict__ mvf, const mpm_params P,
+                                                              const mpm_advect_params adv, const mpm_wall_params W,
+                                                              uint32_t* __restrict__ kill_bits) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t M = adv.diffuse_max;
+    bool kill = false;
+    if (i < M && pool[i].alive != 0u) {
+        mpm_diffuse_particle p = pool[i];
+        const f3 pos3 = mk(p.pos[0], p.pos[1], p.pos[2]);
+        const float dt = P.dt, g = P.gravity;
+        bool dead = false;
+        if (p.ptype == MPM_DIFFUSE_SPRAY) {
+            p.vel[1] += g * dt;
+            p.pos[0] = pos3.x + dt * p.vel[0]; p.pos[1] = pos3.y + dt * p.vel[1]; p.pos[2] = pos3.z + dt * p.vel[2];
+            p.pos[3] = 0.0f;
+        } else if (p.ptype == MPM_DIFFUSE_FOAM) {
+            const f3 gv = sample_grid_velocity(mvf, P, pos3);
+            p.pos[0] = pos3.x + dt * gv.x; p.pos[1] = pos3.y + dt * gv.y; p.pos[2] = pos3.z + dt * gv.z;
+            p.pos[3] = 0.0f;
+            p.lifetime -= dt;
+            if (p.lifetime <= 0.0f) dead = true;
+        } else if (p.ptype == MPM_DIFFUSE_BUBBLE) {
+            const f3 gv = sample_grid_velocity(mvf, P, pos3);
+            p.vel[0] += dt * adv.drag * (gv.x - p.vel[0]);
+            p.vel[1] += dt * (adv.buoyancy * -g + adv.drag * (gv.y - p.vel[1]));
+            p.vel[2] += dt * adv.drag * (gv.z - p.vel[2]);
+            p.pos[0] = pos3.x + dt * p.vel[0]; p.pos[1] = pos3.y + dt * p.vel[1]; p.pos[2] = pos3.z + dt * p.vel[2];
+            p.pos[3] = 0.0f;
+        }
+        if (!dead) {
+            const uint32_t nw = wall_count_of(W.count_pad[0]);
+            for (uint32_t wi = 0; wi < nw; ++wi) {
+                const WallD w = load_wall(W.walls[wi]);
+                const f3 lp = wall_to_local(mk(p.pos[0], p.pos[1], p.pos[2]), w);
+                if (!inside_open(lp, w.mn, w.mx)) continue;
+                f3 nl;
+                const float sw = wall_sdf_normal(lp, w.mn, w.mx, nl);
+                const f3 nn = wall_to_world_dir(nl, w);
+                p.pos[0] = p.pos[0] - nn.x * sw; p.pos[1] = p.pos[1] - nn.y * sw; p.pos[2] = p.pos[2] - nn.z * sw;
+                p.pos[3] = 0.0f;
+                const f3 wvel = wall_vel_at(mk(p.pos[0], p.pos[1], p.pos[2]), w);
+                const f3 vrel = sub(mk(p.vel[0], p.vel[1], p.vel[2]), wvel);
+                const float vn = dot3(vrel, nn);
+                if (vn < 0.0f) {
+                    const float kk = (1.0f + kRestitution) * vn;
+                    const f3 nvr = mk(vrel.x - kk * nn.x, vrel.y - kk * nn.y, vrel.z - kk * nn.z);
+                    p.vel[0] = wvel.x + nvr.x; p.vel[1] = wvel.y + nvr.y; p.vel[2] = wvel.z + nvr.z;
+                    p.vel[3] = 0.0f;
+                }
+            }
+            if (p.pos[1] < P.hard_min) dead = true;
+        }
+        if (dead) {
+            pool[i].alive = 0u;
+            kill = true;
+        } else {
+            reflect_axis(p.pos[0], p.vel[0], P.hard_min, P.hard_max_x);
+            reflect_axis(p.pos[1], p.vel[1], P.hard_min, P.hard_max_y);
+            reflect_axis(p.pos[2], p.vel[2], P.hard_min, P.hard_max_z);
+            p.pos[3] = 0.0f;
+            p.vel[3] = 0.0f;
+            pool[i] = p;
+        }
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, kill);
+    if ((threadIdx.x & 31) == 0 && (i >> 5) < (M + 31u) / 32u) kill_bits[i >> 5] = b;
+}
+
+__global__ void __launch_bounds__(kRankThreads) k_diffuse_kill_push(const uint32_t* __restrict__ bits,
+                                                                     uint32_t nwords,
+                                                                     const uint32_t* __restrict__ counts,
+                                                                     const int32_t* __restrict__ state,
+                                                                     uint32_t* __restrict__ free_list) {
+    const uint32_t w = blockIdx.x * kRankThreads + threadIdx.x;
+    uint32_t word = w < nwords ? bits[w] : 0u;
+    uint32_t r = group_rank_base(word, counts);
+    const int32_t t0 = state[0];
+    while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        free_list[(uint32_t)(t0 + (int32_t)r)] = w * 32u + (uint32_t)b;
+        ++r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launch sequence for one substep (fluid-gpu.js:663-682,
+// diffuse-gpu.js:148-166).
+// ---------------------------------------------------------------------------
+static inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+
+// RAII phase marker: records a start/end event pair when profiling is on.
+struct Phase {
+    Scene& s;
+    int ph;
+    cudaEvent_t a = nullptr;
+    Phase(Scene& sc, int p) : s(sc), ph(p) { s.begin_phase(ph, &a); }
+    ~Phase() { s.end_phase(ph, a); }
+};
+
+cudaError_t launch_substep(Scene& s) {
+    cudaStream_t st = s.stream;
+    const mpm_params& P = s.params;
+    const uint32_t n = P.particle_num;
+    const uint64_t G = s.G;
+    {
+        Phase ph(s, MPM_PHASE_CLEAR);
+        cudaError_t e = cudaMemsetAsync(s.grid_i32, 0, 16 * G, st);   // CLEAR
+        if (e != cudaSuccess) return e;
+    }
+    if (n > 0) {
+        Phase ph(s, MPM_PHASE_P2G_MASS);
+        k_p2g_mass<<<blocks_for(n, kThreads), kThreads, 0, st>>>(s.pos, s.mass, s.cm, n, (int32_t)s.X,
+                                                                 (int32_t)s.Y, (int32_t)s.Z);
+        s.launches++;
+    }
+    {
+        Phase ph(s, MPM_PHASE_DECODE_MASS);
+        k_decode_mass<<<blocks_for(G, kThreads), kThreads, 0, st>>>(s.cm, s.cmf, G);
+        s.launches++;
+    }
+    if (n > 0) {
+        Phase ph(s, MPM_PHASE_P2G_MOM);
+        k_p2g_mom<<<blocks_for(n, kThreads), kThreads, 0, st>>>(s.pos, s.vel, s.aff, s.mass, s.cmf, s.mv, s.dens, P,
+                                                                (uint32_t)G);
+        s.launches++;
+    }
+    {
+        Phase ph(s, MPM_PHASE_UPDATE_GRID);
+        k_update_grid<<<blocks_for(G, kThreads), kThreads, 0, st>>>(s.mv, s.cm, s.mvf, P, s.walls);
+        s.launches++;
+    }
+    if (s.hand_active && s.hand_dims[0] > 0 && s.hand_dims[1] > 0 && s.hand_dims[2] > 0) {
+        Phase ph(s, MPM_PHASE_APPLY_HAND);
+        dim3 grid(blocks_for(s.hand_dims[0], 4), blocks_for(s.hand_dims[1], 4), blocks_for(s.hand_dims[2], 4));
+        k_apply_hand<<<grid, dim3(4, 4, 4), 0, st>>>(s.mvf, P, s.hand);
+        s.launches++;
+    }
+    if (n > 0) {
+        Phase ph(s, MPM_PHASE_G2P);
+        k_g2p<<<blocks_for(n, kThreads), kThreads, 0, st>>>(s.pos, s.vel, s.aff, s.mvf, P, s.walls, (uint32_t)G);
+        s.launches++;
+    }
+    DiffuseState& d = s.diffuse;
+    if (d.enabled) {
+        d.seed = d.seed + 1u;                 // diffuse-gpu.js:149
+        mpm_gen_params gen = d.gen;
+        gen.seed = d.seed;
+        const uint32_t nwords = (n + 31u) / 32u;
+        const uint32_t nb = blocks_for(nwords, kRankThreads);
+        if (n > 0) {
+            Phase ph(s, MPM_PHASE_DIFFUSE_GEN);
+            k_diffuse_gen_eval<<<blocks_for(nwords * 32u, kThreads), kThreads, 0, st>>>(
+                s.pos, s.vel, s.mass, s.dens, s.cmf, P, gen, d.staging, d.spawn_bits);
+            k_bits_count<<<nb, kRankThreads, 0, st>>>(d.spawn_bits, nwords, d.block_counts);
+            k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, nb, d.top, d.rank_state, 0);
+            k_diffuse_gen_write<<<nb, kRankThreads, 0, st>>>(d.spawn_bits, nwords, d.block_counts, d.rank_state,
+                                                              d.free_list, d.staging, d.pool);
+            s.launches += 4;
+        }
+        const uint32_t M = d.max_count;
+        const uint32_t mwords = (M + 31u) / 32u;
+        const uint32_t mb = blocks_for(mwords, kRankThreads);
+        mpm_advect_params adv = d.adv;
+        adv.diffuse_max = M;
+        {
+            Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
+            k_diffuse_advect<<<blocks_for(mwords * 32u, kThreads), kThreads, 0, st>>>(d.pool, s.mvf, P, adv,
+                                                                                       s.walls, d.kill_bits);
+            k_bits_count<<<mb, kRankThreads, 0, st>>>(d.kill_bits, mwords, d.block_counts);
+            k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mb, d.top, d.rank_state, 1);
+            k_diffuse_kill_push<<<mb, kRankThreads, 0, st>>>(d.kill_bits, mwords, d.block_counts, d.rank_state,
+                                                              d.free_list);
+            s.launches += 4;
+        }
+    }
+    s.substeps_done++;
+    return cudaGetLastError();
+}
+
+}  // namespace mpm

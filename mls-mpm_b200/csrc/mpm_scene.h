@@ -1,0 +1,88 @@
+// mpm_scene.h — host-side scene object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm_b200.h"
+
+namespace mpm {
+
+// Scratch sizes for the deterministic free-list ranking (bitmask + per-block
+// popcounts + one scan).  kBitsPerBlock ids are covered by one rank block.
+constexpr uint32_t kRankThreads = 256;                 // words per rank block
+constexpr uint32_t kBitsPerBlock = kRankThreads * 32;  // ids per rank block
+
+struct DiffuseState {
+    bool enabled = false;
+    uint32_t max_count = 0;
+    mpm_gen_params gen{};       // last _writeGenParams contents
+    mpm_advect_params adv{};
+    uint32_t seed = 1;          // DiffuseGPU._seed (diffuse-gpu.js:31)
+    mpm_diffuse_particle* pool = nullptr;   // M x 48 B
+    uint32_t* free_list = nullptr;          // M
+    int32_t* top = nullptr;                 // 1 (device)
+    // ranking scratch
+    uint32_t* spawn_bits = nullptr;         // ceil(N/32) words, one bit per fluid particle id
+    uint32_t* kill_bits = nullptr;          // ceil(M/32) words, one bit per slot
+    uint32_t* block_counts = nullptr;       // max(ceil(N/8192), ceil(M/8192)) + 1
+    int32_t* rank_state = nullptr;          // [0] = top before the pass, [1] = total, [2] = applied
+    mpm_diffuse_particle* staging = nullptr;  // N x 48 B spawn records indexed by particle id
+    int32_t* host_top = nullptr;            // pinned 4 B for alive-count readback
+};
+
+struct Scene {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t X = 0, Y = 0, Z = 0;
+    uint64_t G = 0;
+    uint32_t capacity = 0;
+    uint32_t n_active = 0;
+
+    mpm_params params{};
+    mpm_wall_params walls{};
+    mpm_hand_params hand{};
+    int hand_active = 0;
+    int32_t hand_dims[3] = {0, 0, 0};
+
+    // particle buffers, reference layout
+    float4* pos = nullptr;
+    float4* vel = nullptr;
+    float* aff = nullptr;
+    float* mass = nullptr;
+    float* dens = nullptr;
+    // grid buffers, reference layout; cm and mv share one allocation
+    int32_t* grid_i32 = nullptr;   // [cm: G][mv: 3G]
+    int32_t* cm = nullptr;
+    int32_t* mv = nullptr;
+    float* cmf = nullptr;
+    float* mvf = nullptr;
+
+    DiffuseState diffuse;
+    uint64_t substeps_done = 0;
+    uint64_t launches = 0;
+
+    // per-phase CUDA-event profiler (mpm_profile_enable)
+    struct Pending { int phase; cudaEvent_t a, b; };
+    bool profile = false;
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<Pending> pending;
+    double prof_ms[MPM_PHASE_COUNT] = {};
+    uint64_t prof_n[MPM_PHASE_COUNT] = {};
+
+    cudaEvent_t take_event();
+    void begin_phase(int phase, cudaEvent_t* a);
+    void end_phase(int phase, cudaEvent_t a);
+    cudaError_t drain_profile();
+};
+
+void set_error(const std::string& msg);
+
+}  // namespace mpm
+
+struct mpm_scene {
+    mpm::Scene s;
+};
