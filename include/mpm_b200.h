@@ -63,12 +63,17 @@ typedef enum mpm_buffer {
     MPM_BUF_FREE_TOP = 11       /* DiffuseGPU.freeListTopBuffer i32    */
 } mpm_buffer;
 
+/* mpm_desc.flags: run the plain engine (one kernel per reference pass on
+ * reference-layout buffers) instead of the binned engine.  Both give the
+ * same bits; the plain engine exists as a cross-check and for debugging. */
+#define MPM_FLAG_PLAIN 1u
+
 /* Scene creation descriptor (FluidGPU constructor, fluid-gpu.js:10-17). */
 typedef struct mpm_desc {
     uint32_t grid_X, grid_Y, grid_Z;  /* cells */
     uint32_t particle_capacity;       /* particleNum: buffer capacity */
     int32_t device;                   /* CUDA device ordinal */
-    uint32_t flags;                   /* reserved, 0 */
+    uint32_t flags;                   /* MPM_FLAG_* */
 } mpm_desc;
 
 typedef struct mpm_scene mpm_scene;

@@ -101,6 +101,7 @@ static void free_scene(Scene& s) {
     for (cudaEvent_t e : s.event_pool) cudaEventDestroy(e);
     s.pending.clear();
     s.event_pool.clear();
+    fast_free(s.fast);
     void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
                     s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
                     s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.rank_state, s.diffuse.staging};
@@ -129,8 +130,10 @@ static bool buffer_info(Scene& s, mpm_buffer which, void** ptr, size_t* bytes) {
         case MPM_BUF_AFFINE: *ptr = s.aff; *bytes = N * 36; return true;
         case MPM_BUF_MASS: *ptr = s.mass; *bytes = N * 4; return true;
         case MPM_BUF_DENSITY: *ptr = s.dens; *bytes = N * 4; return true;
-        case MPM_BUF_CELL_MV: *ptr = s.mv; *bytes = G * 12; return true;
-        case MPM_BUF_CELL_MASS: *ptr = s.cm; *bytes = G * 4; return true;
+        case MPM_BUF_CELL_MV:
+            *ptr = s.engine == kEnginePlain ? s.mv : s.fast.cm_current + G; *bytes = G * 12; return true;
+        case MPM_BUF_CELL_MASS:
+            *ptr = s.engine == kEnginePlain ? s.cm : s.fast.cm_current; *bytes = G * 4; return true;
         case MPM_BUF_CELL_MV_F32: *ptr = s.mvf; *bytes = G * 12; return true;
         case MPM_BUF_CELL_MASS_F32: *ptr = s.cmf; *bytes = G * 4; return true;
         case MPM_BUF_DIFFUSE:
@@ -144,6 +147,34 @@ static bool buffer_info(Scene& s, mpm_buffer which, void** ptr, size_t* bytes) {
             *ptr = s.diffuse.top; *bytes = 4; return true;
     }
     return false;
+}
+
+static bool is_particle_buffer(mpm_buffer w) {
+    return w == MPM_BUF_POS || w == MPM_BUF_VEL || w == MPM_BUF_AFFINE || w == MPM_BUF_MASS || w == MPM_BUF_DENSITY;
+}
+
+// Binned engine: bring the reference-layout particle buffers up to date.
+static cudaError_t sync_reference_buffers(Scene& s) {
+    if (s.engine != kEngineBinned || !s.ref_stale) return cudaSuccess;
+    cudaError_t e = fast_export(s.fast, s.pos, s.vel, s.aff, s.mass, s.fast.dens_valid ? s.dens : nullptr, s.stream);
+    if (e == cudaSuccess) s.ref_stale = false;
+    return e;
+}
+
+// Binned engine: (re)load the working state from the reference-layout buffers.
+static cudaError_t import_state(Scene& s) {
+    cudaError_t e = fast_import(s.fast, s.pos, s.vel, s.aff, s.mass, s.params.particle_num, s.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.cmf, 0, s.G * 4, s.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.mvf, 0, s.G * 12, s.stream);
+    if (e == cudaSuccess) s.fast_stale = false;
+    return e;
+}
+
+static cudaError_t launch_substep(Scene& s) {
+    s.substeps_done++;
+    if (s.engine == kEnginePlain) return launch_substep_plain(s);
+    s.ref_stale = true;
+    return fast_substep(s);
 }
 
 }  // namespace mpm
@@ -237,6 +268,7 @@ mpm_status mpm_create(const mpm_desc* d, mpm_scene** out) {
     s.device = d->device;
     s.X = d->grid_X; s.Y = d->grid_Y; s.Z = d->grid_Z; s.G = G;
     s.capacity = d->particle_capacity;
+    s.engine = (d->flags & MPM_FLAG_PLAIN) ? kEnginePlain : kEngineBinned;
     mpm_desc dd = *d;
     mpm_default_params(&dd, &s.params);
     cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
@@ -246,7 +278,8 @@ mpm_status mpm_create(const mpm_desc* d, mpm_scene** out) {
     if (e == cudaSuccess) e = dalloc(&s.aff, N * 36);
     if (e == cudaSuccess) e = dalloc(&s.mass, N * 4);
     if (e == cudaSuccess) e = dalloc(&s.dens, N * 4);
-    if (e == cudaSuccess) e = dalloc(&s.grid_i32, G * 16);
+    if (e == cudaSuccess && s.engine == kEnginePlain) e = dalloc(&s.grid_i32, G * 16);
+    if (e == cudaSuccess && s.engine == kEngineBinned) e = fast_alloc(s.fast, s.X, s.Y, s.Z, s.capacity, s.device);
     if (e == cudaSuccess) e = dalloc(&s.cmf, G * 4);
     if (e == cudaSuccess) e = dalloc(&s.mvf, G * 12);
     if (e != cudaSuccess) {
@@ -254,15 +287,18 @@ mpm_status mpm_create(const mpm_desc* d, mpm_scene** out) {
         delete sc;
         return cuda_fail(e, "mpm_create allocation");
     }
-    s.cm = s.grid_i32;
-    s.mv = s.grid_i32 + G;
+    if (s.grid_i32) {
+        s.cm = s.grid_i32;
+        s.mv = s.grid_i32 + G;
+    }
     // WebGPU zero-fills new buffers (fluid-gpu.js:226-227)
     cudaMemsetAsync(s.pos, 0, N * 16, s.stream);
     cudaMemsetAsync(s.vel, 0, N * 16, s.stream);
     cudaMemsetAsync(s.aff, 0, N * 36, s.stream);
     cudaMemsetAsync(s.mass, 0, N * 4, s.stream);
     cudaMemsetAsync(s.dens, 0, N * 4, s.stream);
-    cudaMemsetAsync(s.grid_i32, 0, G * 16, s.stream);
+    if (s.grid_i32) cudaMemsetAsync(s.grid_i32, 0, G * 16, s.stream);
+    if (s.engine == kEngineBinned) fast_import(s.fast, s.pos, s.vel, s.aff, s.mass, 0, s.stream);
     cudaMemsetAsync(s.cmf, 0, G * 4, s.stream);
     cudaMemsetAsync(s.mvf, 0, G * 12, s.stream);
     e = cudaStreamSynchronize(s.stream);
@@ -297,9 +333,13 @@ mpm_status mpm_upload_particles(mpm_scene* sc, const float* pos4, const float* v
     if (aff9) CUDA_TRY(cudaMemcpyAsync(s.aff, aff9, (size_t)n * 36, cudaMemcpyHostToDevice, st), "upload affine");
     else CUDA_TRY(cudaMemsetAsync(s.aff, 0, (size_t)n * 36, st), "zero affine");
     CUDA_TRY(cudaMemcpyAsync(s.mass, mass, (size_t)n * 4, cudaMemcpyHostToDevice, st), "upload mass");
-    CUDA_TRY(cudaStreamSynchronize(st), "upload sync");
     s.n_active = n;
     s.params.particle_num = n;
+    if (s.engine == kEngineBinned) {
+        s.ref_stale = false;
+        CUDA_TRY(import_state(s), "import");
+    }
+    CUDA_TRY(cudaStreamSynchronize(st), "upload sync");
     return MPM_OK;
 }
 
@@ -309,6 +349,12 @@ mpm_status mpm_set_params(mpm_scene* sc, const mpm_params* p) {
     if (p->grid_X != s.X || p->grid_Y != s.Y || p->grid_Z != s.Z)
         return fail(MPM_ERR_INVALID_ARG, "params grid dims differ from the scene's");
     if (p->particle_num > s.capacity) return fail(MPM_ERR_CAPACITY, "particle_num exceeds capacity");
+    if (s.engine == kEngineBinned && p->particle_num != s.fast.n) {
+        // active count changed (spawn / delete): reload the working state next step
+        DeviceGuard guard(s.device);
+        CUDA_TRY(sync_reference_buffers(s), "export");
+        s.fast_stale = true;
+    }
     s.params = *p;
     s.n_active = p->particle_num;
     return MPM_OK;
@@ -379,6 +425,10 @@ mpm_status mpm_step(mpm_scene* sc, int substeps) {
     if (!sc || substeps < 0) return fail(MPM_ERR_INVALID_ARG, "bad argument");
     Scene& s = sc->s;
     DeviceGuard guard(s.device);
+    if (s.engine == kEngineBinned && s.fast_stale) {
+        cudaError_t e = import_state(s);
+        if (e != cudaSuccess) return cuda_fail(e, "import");
+    }
     for (int i = 0; i < substeps; ++i) {
         cudaError_t e = launch_substep(s);
         if (e != cudaSuccess) return cuda_fail(e, "mpm_step launch");
@@ -396,6 +446,10 @@ mpm_status mpm_sync(mpm_scene* sc) {
 mpm_status mpm_get_buffer(mpm_scene* sc, mpm_buffer which, void** dev_ptr, size_t* bytes) {
     if (!sc || !dev_ptr || !bytes) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     if (!buffer_info(sc->s, which, dev_ptr, bytes)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
+    if (is_particle_buffer(which)) {
+        DeviceGuard guard(sc->s.device);
+        CUDA_TRY(sync_reference_buffers(sc->s), "export");
+    }
     return MPM_OK;
 }
 
@@ -406,6 +460,7 @@ mpm_status mpm_download(mpm_scene* sc, mpm_buffer which, void* host_dst, size_t 
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
     DeviceGuard guard(sc->s.device);
+    if (is_particle_buffer(which)) CUDA_TRY(sync_reference_buffers(sc->s), "export");
     CUDA_TRY(cudaMemcpyAsync(host_dst, p, bytes, cudaMemcpyDeviceToHost, sc->s.stream), "download");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "download sync");
     return MPM_OK;
@@ -418,6 +473,10 @@ mpm_status mpm_upload(mpm_scene* sc, mpm_buffer which, const void* host_src, siz
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
     DeviceGuard guard(sc->s.device);
+    if (is_particle_buffer(which)) {
+        CUDA_TRY(sync_reference_buffers(sc->s), "export");
+        if (sc->s.engine == kEngineBinned) sc->s.fast_stale = true;
+    }
     CUDA_TRY(cudaMemcpyAsync(p, host_src, bytes, cudaMemcpyHostToDevice, sc->s.stream), "upload");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "upload sync");
     return MPM_OK;
@@ -470,7 +529,7 @@ mpm_status mpm_profile_read(mpm_scene* sc, double* ms, uint64_t* count, int rese
 
 mpm_status mpm_launch_count(mpm_scene* sc, uint64_t* launches) {
     if (!sc || !launches) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
-    *launches = sc->s.launches;
+    *launches = sc->s.launches + sc->s.fast.launches;
     return MPM_OK;
 }
 

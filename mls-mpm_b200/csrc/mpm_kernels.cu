@@ -517,7 +517,8 @@ __global__ void __launch_bounds__(kRankThreads) k_diffuse_gen_write(const uint32
                                                                      const int32_t* __restrict__ state,
                                                                      const uint32_t* __restrict__ free_list,
                                                                      const mpm_diffuse_particle* __restrict__ staging,
-                                                                     mpm_diffuse_particle* __restrict__ pool) {
+                                                                     mpm_diffuse_particle* __restrict__ pool,
+                                                                     uint32_t M) {
     const uint32_t w = blockIdx.x * kRankThreads + threadIdx.x;
     uint32_t word = w < nwords ? bits[w] : 0u;
     uint32_t r = group_rank_base(word, counts);
@@ -525,9 +526,11 @@ __global__ void __launch_bounds__(kRankThreads) k_diffuse_gen_write(const uint32
     while (word) {
         const int b = __ffs(word) - 1;
         word &= word - 1;
-        if ((int32_t)r < applied) {
-            const uint32_t slot = free_list[(uint32_t)(t0 - 1 - (int32_t)r)];
-            pool[slot] = staging[w * 32u + (uint32_t)b];
+        const int32_t fi = t0 - 1 - (int32_t)r;
+        // free-list state uploaded by a caller may be inconsistent: never index outside the pool
+        if ((int32_t)r < applied && fi >= 0 && (uint32_t)fi < M) {
+            const uint32_t slot = free_list[fi];
+            if (slot < M) pool[slot] = staging[w * 32u + (uint32_t)b];
         }
         ++r;
     }
@@ -652,7 +655,7 @@ __global__ void __launch_bounds__(kRankThreads) k_diffuse_kill_push(const uint32
                                                                      uint32_t nwords,
                                                                      const uint32_t* __restrict__ counts,
                                                                      const int32_t* __restrict__ state,
-                                                                     uint32_t* __restrict__ free_list) {
+                                                                     uint32_t* __restrict__ free_list, uint32_t M) {
     const uint32_t w = blockIdx.x * kRankThreads + threadIdx.x;
     uint32_t word = w < nwords ? bits[w] : 0u;
     uint32_t r = group_rank_base(word, counts);
@@ -660,7 +663,8 @@ __global__ void __launch_bounds__(kRankThreads) k_diffuse_kill_push(const uint32
     while (word) {
         const int b = __ffs(word) - 1;
         word &= word - 1;
-        free_list[(uint32_t)(t0 + (int32_t)r)] = w * 32u + (uint32_t)b;
+        const int32_t fi = t0 + (int32_t)r;
+        if (fi >= 0 && (uint32_t)fi < M) free_list[fi] = w * 32u + (uint32_t)b;
         ++r;
     }
 }
@@ -671,16 +675,62 @@ __global__ void __launch_bounds__(kRankThreads) k_diffuse_kill_push(const uint32
 // ---------------------------------------------------------------------------
 static inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
-// RAII phase marker: records a start/end event pair when profiling is on.
-struct Phase {
-    Scene& s;
-    int ph;
-    cudaEvent_t a = nullptr;
-    Phase(Scene& sc, int p) : s(sc), ph(p) { s.begin_phase(ph, &a); }
-    ~Phase() { s.end_phase(ph, a); }
-};
+cudaError_t launch_apply_hand(Scene& s) {
+    dim3 grid(blocks_for(s.hand_dims[0], 4), blocks_for(s.hand_dims[1], 4), blocks_for(s.hand_dims[2], 4));
+    k_apply_hand<<<grid, dim3(4, 4, 4), 0, s.stream>>>(s.mvf, s.params, s.hand);
+    return cudaGetLastError();
+}
 
-cudaError_t launch_substep(Scene& s) {
+// DiffuseGPU.step (diffuse-gpu.js:148-166) after G2P.  With eval the spawn
+// decision pass runs here (plain engine); the binned engine makes that
+// decision in its G2P epilogue and has already bumped the seed.
+cudaError_t launch_diffuse(Scene& s, bool eval) {
+    cudaStream_t st = s.stream;
+    const mpm_params& P = s.params;
+    DiffuseState& d = s.diffuse;
+    const uint32_t n = P.particle_num;
+    const uint32_t nwords = (n + 31u) / 32u;
+    const uint32_t nb = blocks_for(nwords, kRankThreads);
+    if (eval) {
+        d.seed = d.seed + 1u;                 // diffuse-gpu.js:149
+        mpm_gen_params gen = d.gen;
+        gen.seed = d.seed;
+        if (n > 0) {
+            Phase ph(s, MPM_PHASE_DIFFUSE_GEN);
+            k_diffuse_gen_eval<<<blocks_for(nwords * 32u, kThreads), kThreads, 0, st>>>(
+                s.pos, s.vel, s.mass, s.dens, s.cmf, P, gen, d.staging, d.spawn_bits);
+            s.launches++;
+        }
+    }
+    if (n > 0) {
+        Phase ph(s, MPM_PHASE_DIFFUSE_GEN);
+        k_bits_count<<<nb, kRankThreads, 0, st>>>(d.spawn_bits, nwords, d.block_counts);
+        k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, nb, d.top, d.rank_state, 0);
+        k_diffuse_gen_write<<<nb, kRankThreads, 0, st>>>(d.spawn_bits, nwords, d.block_counts, d.rank_state,
+                                                          d.free_list, d.staging, d.pool, d.max_count);
+        s.launches += 3;
+    }
+    const uint32_t M = d.max_count;
+    const uint32_t mwords = (M + 31u) / 32u;
+    const uint32_t mb = blocks_for(mwords, kRankThreads);
+    mpm_advect_params adv = d.adv;
+    adv.diffuse_max = M;
+    {
+        Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
+        k_diffuse_advect<<<blocks_for(mwords * 32u, kThreads), kThreads, 0, st>>>(d.pool, s.mvf, P, adv, s.walls,
+                                                                                   d.kill_bits);
+        k_bits_count<<<mb, kRankThreads, 0, st>>>(d.kill_bits, mwords, d.block_counts);
+        k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mb, d.top, d.rank_state, 1);
+        k_diffuse_kill_push<<<mb, kRankThreads, 0, st>>>(d.kill_bits, mwords, d.block_counts, d.rank_state,
+                                                          d.free_list, M);
+        s.launches += 4;
+    }
+    return cudaGetLastError();
+}
+
+// One substep of the plain engine: one kernel per reference pass, in the
+// reference's order (fluid-gpu.js:663-682), on reference-layout buffers.
+cudaError_t launch_substep_plain(Scene& s) {
     cudaStream_t st = s.stream;
     const mpm_params& P = s.params;
     const uint32_t n = P.particle_num;
@@ -714,8 +764,8 @@ cudaError_t launch_substep(Scene& s) {
     }
     if (s.hand_active && s.hand_dims[0] > 0 && s.hand_dims[1] > 0 && s.hand_dims[2] > 0) {
         Phase ph(s, MPM_PHASE_APPLY_HAND);
-        dim3 grid(blocks_for(s.hand_dims[0], 4), blocks_for(s.hand_dims[1], 4), blocks_for(s.hand_dims[2], 4));
-        k_apply_hand<<<grid, dim3(4, 4, 4), 0, st>>>(s.mvf, P, s.hand);
+        cudaError_t e = launch_apply_hand(s);
+        if (e != cudaSuccess) return e;
         s.launches++;
     }
     if (n > 0) {
@@ -723,41 +773,10 @@ cudaError_t launch_substep(Scene& s) {
         k_g2p<<<blocks_for(n, kThreads), kThreads, 0, st>>>(s.pos, s.vel, s.aff, s.mvf, P, s.walls, (uint32_t)G);
         s.launches++;
     }
-    DiffuseState& d = s.diffuse;
-    if (d.enabled) {
-        d.seed = d.seed + 1u;                 // diffuse-gpu.js:149
-        mpm_gen_params gen = d.gen;
-        gen.seed = d.seed;
-        const uint32_t nwords = (n + 31u) / 32u;
-        const uint32_t nb = blocks_for(nwords, kRankThreads);
-        if (n > 0) {
-            Phase ph(s, MPM_PHASE_DIFFUSE_GEN);
-            k_diffuse_gen_eval<<<blocks_for(nwords * 32u, kThreads), kThreads, 0, st>>>(
-                s.pos, s.vel, s.mass, s.dens, s.cmf, P, gen, d.staging, d.spawn_bits);
-            k_bits_count<<<nb, kRankThreads, 0, st>>>(d.spawn_bits, nwords, d.block_counts);
-            k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, nb, d.top, d.rank_state, 0);
-            k_diffuse_gen_write<<<nb, kRankThreads, 0, st>>>(d.spawn_bits, nwords, d.block_counts, d.rank_state,
-                                                              d.free_list, d.staging, d.pool);
-            s.launches += 4;
-        }
-        const uint32_t M = d.max_count;
-        const uint32_t mwords = (M + 31u) / 32u;
-        const uint32_t mb = blocks_for(mwords, kRankThreads);
-        mpm_advect_params adv = d.adv;
-        adv.diffuse_max = M;
-        {
-            Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
-            k_diffuse_advect<<<blocks_for(mwords * 32u, kThreads), kThreads, 0, st>>>(d.pool, s.mvf, P, adv,
-                                                                                       s.walls, d.kill_bits);
-            k_bits_count<<<mb, kRankThreads, 0, st>>>(d.kill_bits, mwords, d.block_counts);
-            k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mb, d.top, d.rank_state, 1);
-            k_diffuse_kill_push<<<mb, kRankThreads, 0, st>>>(d.kill_bits, mwords, d.block_counts, d.rank_state,
-                                                              d.free_list);
-            s.launches += 4;
-        }
-    }
-    s.substeps_done++;
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (s.diffuse.enabled) e = launch_diffuse(s, /*eval=*/true);
+    return e;
 }
 
 }  // namespace mpm

@@ -1,4 +1,4 @@
-// mpm_kernels.h — launch entry points of the substep kernels.
+// mpm_kernels.h — launchers of the per-pass kernels.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -7,7 +7,13 @@
 
 namespace mpm {
 
-// Enqueue one substep (fluid passes + diffuse when enabled) on s.stream.
-cudaError_t launch_substep(Scene& s);
+// One substep of the plain engine (one kernel per reference pass).
+cudaError_t launch_substep_plain(Scene& s);
+
+// APPLY_HAND over the scene's hand box (both engines).
+cudaError_t launch_apply_hand(Scene& s);
+
+// DiffuseGPU.step after G2P; eval = run the spawn-decision pass here.
+cudaError_t launch_diffuse(Scene& s, bool eval);
 
 }  // namespace mpm

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/mpm_b200.h"
+#include "mpm_fast.h"
 
 namespace mpm {
 
@@ -34,8 +35,13 @@ struct DiffuseState {
     int32_t* host_top = nullptr;            // pinned 4 B for alive-count readback
 };
 
+// Engines: the binned item-major substep (default) and the plain per-pass
+// substep (MPM_FLAG_PLAIN), which mirrors the reference's dispatch list.
+enum Engine { kEngineBinned = 0, kEnginePlain = 1 };
+
 struct Scene {
     int device = 0;
+    int engine = kEngineBinned;
     cudaStream_t stream = nullptr;
     uint32_t X = 0, Y = 0, Z = 0;
     uint64_t G = 0;
@@ -62,6 +68,10 @@ struct Scene {
     float* mvf = nullptr;
 
     DiffuseState diffuse;
+    FastEngine fast;
+    // binned engine: which copy of the particle state is newer
+    bool ref_stale = false;    // reference-layout buffers behind the binned state
+    bool fast_stale = false;   // binned state behind the reference-layout buffers
     uint64_t substeps_done = 0;
     uint64_t launches = 0;
 
@@ -80,6 +90,15 @@ struct Scene {
 };
 
 void set_error(const std::string& msg);
+
+// RAII phase marker: records a start/end event pair when profiling is on.
+struct Phase {
+    Scene& s;
+    int ph;
+    cudaEvent_t a = nullptr;
+    Phase(Scene& sc, int p) : s(sc), ph(p) { s.begin_phase(ph, &a); }
+    ~Phase() { s.end_phase(ph, a); }
+};
 
 }  // namespace mpm
 

@@ -23,14 +23,14 @@ def cpu_run(scenario, impl="oracle", threads=1):
 class GpuScene:
     """A scene driven through the raw C ABI."""
 
-    def __init__(self, lib, scene, diffuse_max=0, device=0):
+    def __init__(self, lib, scene, diffuse_max=0, device=0, flags=0):
         self.lib = lib
         self.scene = scene
         self.n = scene.n
         X, Y, Z = scene.grid
         self.G = X * Y * Z
         self.M = diffuse_max
-        d = Desc(X, Y, Z, scene.n, device, 0)
+        d = Desc(X, Y, Z, scene.n, device, flags)
         self.h = ctypes.c_void_p()
         check(lib.mpm_create(ctypes.byref(d), ctypes.byref(self.h)), "mpm_create")
         check(lib.mpm_upload_particles(self.h, abi.ptr(scene.pos), abi.ptr(scene.vel), abi.ptr(scene.affine),
@@ -72,8 +72,11 @@ class GpuScene:
             self.h = None
 
 
-def gpu_run(lib, scenario):
-    g = GpuScene(lib, scenario.scene, scenario.diffuse_max)
+ENGINES = {"binned": 0, "plain": 1}
+
+
+def gpu_run(lib, scenario, engine="binned"):
+    g = GpuScene(lib, scenario.scene, scenario.diffuse_max, flags=ENGINES[engine])
     try:
         for P, W, H, dims, gen, adv in scenario.frames():
             g.frame(P, W, H, dims)

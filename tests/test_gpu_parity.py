@@ -23,19 +23,21 @@ REL_TOL = 1e-5
 GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")))
 
 
+@pytest.mark.parametrize("engine", ["binned", "plain"])
 @pytest.mark.parametrize("name", sorted(scenarios.SCENARIOS))
-def test_gpu_matches_oracle_every_substep(gpu, name):
+def test_gpu_matches_oracle_every_substep(gpu, name, engine):
     sc = scenarios.SCENARIOS[name]()
-    for s, (g, o) in enumerate(zip(gpu_run(gpu, sc), cpu_run(sc, "oracle", threads=8))):
+    for s, (g, o) in enumerate(zip(gpu_run(gpu, sc, engine), cpu_run(sc, "oracle", threads=8))):
         bad = diff_report(g, o)
-        assert not bad, f"{name} substep {s}: {bad}"
+        assert not bad, f"{name} [{engine}] substep {s}: {bad}"
 
 
+@pytest.mark.parametrize("engine", ["binned", "plain"])
 @pytest.mark.parametrize("name", sorted(scenarios.SCENARIOS))
-def test_gpu_matches_reference_golden(gpu, name):
+def test_gpu_matches_reference_golden(gpu, name, engine):
     sc = scenarios.SCENARIOS[name]()
     gold = GOLDEN["scenarios"][name]["steps"]
-    for s, g in enumerate(gpu_run(gpu, sc)):
+    for s, g in enumerate(gpu_run(gpu, sc, engine)):
         d = O.digest(g)
         bad = [k for k, v in gold[s]["digest"].items() if d.get(k) != v]
         assert not bad, f"{name} substep {s}: {bad}"
