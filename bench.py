@@ -104,21 +104,23 @@ def dist_setup():
     return ws, rank, local
 
 
-def cpu_reference_rate(scene, substeps, threads, budget_s=None):
+def cpu_reference_rate(scene, substeps, threads, budget_s=None, warmup=1):
     """Times the reference pin (the reference's WGSL compiled on the host) or,
     when it is absent, the oracle restatement, over `substeps` substeps of
-    `scene` with diffuse.  Returns (updates/s, kind, steps run, seconds)."""
+    `scene` with diffuse after `warmup` untimed ones.  Returns (updates/s,
+    kind, steps run, seconds)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle as O
     import scenarios
     kind = "reference" if O.ref_available() else "port"
     impl = "ref" if kind == "reference" else "oracle"
-    sc = scenarios.Scenario(scene.name, scene, substeps + 1, diffuse_max=scene.diffuse_max)
+    sc = scenarios.Scenario(scene.name, scene, substeps + warmup, diffuse_max=scene.diffuse_max)
     st = O.new_state(scene, scene.diffuse_max)
     frames = sc.frames()
-    P, W, H, dims, gen, adv = next(frames)
-    O.substep(st, P, W, H, dims, gen, adv, threads=threads, impl=impl)    # warm caches
+    for _ in range(warmup):
+        P, W, H, dims, gen, adv = next(frames)
+        O.substep(st, P, W, H, dims, gen, adv, threads=threads, impl=impl)
     t0 = time.perf_counter()
     done = 0
     for P, W, H, dims, gen, adv in frames:
@@ -138,8 +140,7 @@ def run_reference_arm(args, ws, rank):
     scene = scenes.dam_break_1m(0)
     # warm-up steps are untimed; each timed step is one full substep of the
     # scene; the run is capped at ~240 s of CPU time (the sample is stated)
-    rate_w, kind, _, _ = cpu_reference_rate(scene, max(1, args.warmup), threads)
-    rate, kind, done, secs = cpu_reference_rate(scene, args.steps, threads, budget_s=240.0)
+    rate, kind, done, secs = cpu_reference_rate(scene, args.steps, threads, budget_s=240.0, warmup=args.warmup)
     sample = f"{done} substeps of the {WORKLOAD} scene (1,048,576 particles + 262,144 diffuse pool) " \
              f"on {threads} host threads"
     line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
@@ -180,12 +181,18 @@ def main():
     from mls_mpm_b200 import DiffuseGPU, FluidGPU, scenes
     from mls_mpm_b200.abi import check
     scene = scenes.WORKLOADS[args.workload](seed=rank)
-    fl = FluidGPU.from_scene(scene, device=local)
-    DiffuseGPU(scene.diffuse_max).initGPU(local, fl)
-    lib, h = fl._lib, fl._scene
-    sptr = ctypes.c_void_p()
-    check(lib.mpm_get_stream(h, ctypes.byref(sptr)), "mpm_get_stream")
-    stream = torch.cuda.ExternalStream(sptr.value, device=torch.device("cuda", local))
+
+    def make():
+        """One simulation of the workload; three identical copies follow the
+        same trajectory, so the device-timed, per-phase and end-to-end
+        numbers all cover the same substeps [W, W+K)."""
+        fl = FluidGPU.from_scene(scene, device=local)
+        if scene.diffuse_max:
+            DiffuseGPU(scene.diffuse_max).initGPU(local, fl)
+        for _ in range(args.warmup):
+            fl.simFrame()
+        fl.sync()
+        return fl
 
     def barrier():
         if dist is not None:
@@ -198,60 +205,65 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def launches():
-        c = ctypes.c_uint64()
-        lib.mpm_launch_count(h, ctypes.byref(c))
-        return c.value
-
-    # warm-up
-    for _ in range(args.warmup):
-        fl.simFrame()
-    fl.sync()
-    torch.cuda.synchronize()
-
-    # timed region: exactly K substeps, inputs resident in HBM
     clocks = ClockSampler(local)
+    # (1) device-timed region: exactly K substeps, inputs resident in HBM
+    fl = make()
+    lib, h = fl._lib, fl._scene
+    sptr = ctypes.c_void_p()
+    check(lib.mpm_get_stream(h, ctypes.byref(sptr)), "mpm_get_stream")
+    stream = torch.cuda.ExternalStream(sptr.value, device=torch.device("cuda", local))
+    c0, c1 = ctypes.c_uint64(), ctypes.c_uint64()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    l0 = launches()
+    lib.mpm_launch_count(h, ctypes.byref(c0))
     with clocks:
         e0.record(stream)
         for _ in range(args.steps):
             check(lib.mpm_step(h, 1), "mpm_step")
         e1.record(stream)
         e1.synchronize()
-        torch.cuda.synchronize()
-        barrier()
-        ms = max_over_ranks(e0.elapsed_time(e1))
-        n_launch = launches() - l0
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    lib.mpm_launch_count(h, ctypes.byref(c1))
+    n_launch = c1.value - c0.value
+    fl.destroy()
 
-        # per-phase device time over the same workload (CUDA events on the scene stream)
-        prof_steps = min(args.steps, 100)
-        lib.mpm_profile_enable(h, 1)
-        lib.mpm_profile_read(h, None, None, 1)
-        for _ in range(prof_steps):
-            check(lib.mpm_step(h, 1), "mpm_step")
-        pm = (ctypes.c_double * 10)()
-        pc = (ctypes.c_uint64 * 10)()
-        check(lib.mpm_profile_read(h, pm, pc, 1), "mpm_profile_read")
-        lib.mpm_profile_enable(h, 0)
+    # (2) per-phase device time over the same substeps (CUDA events on the scene stream)
+    fl = make()
+    lib, h = fl._lib, fl._scene
+    lib.mpm_profile_enable(h, 1)
+    lib.mpm_profile_read(h, None, None, 1)
+    for _ in range(args.steps):
+        check(lib.mpm_step(h, 1), "mpm_step")
+    pm = (ctypes.c_double * 10)()
+    pc = (ctypes.c_uint64 * 10)()
+    check(lib.mpm_profile_read(h, pm, pc, 1), "mpm_profile_read")
+    names = [lib.mpm_phase_name(i).decode() for i in range(10)]
+    fl.destroy()
 
-        # end to end through the public API: per step the host writes the
-        # frame's uniforms (params, walls, hand: fluid-gpu.js:295-328,
-        # 337-413, 479-527) and reads back the diffuse alive count
-        # (diffuse-gpu.js:172-188), synchronously, like the reference's frame.
-        barrier()
-        t0 = time.perf_counter()
-        for s in range(args.steps):
-            fl.updateHand([40.0, 60.0, 40.0], [0.0, 0.0, 0.0], 4.0, 1.0, False, [40.0, 60.0, 140.0])
-            fl._params_prev = None
-            fl._walls.prev_buf[:] = np.nan
-            fl.simFrame()
+    # (3) end to end through the public API over the same substeps: per step
+    # the host writes the frame's uniforms (params, walls, hand:
+    # fluid-gpu.js:295-328, 337-413, 479-527) and reads back the diffuse alive
+    # count (diffuse-gpu.js:172-188), synchronously, like the reference's frame.
+    fl = make()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fl.updateHand([40.0, 60.0, 40.0], [0.0, 0.0, 0.0], 4.0, 1.0, False, [40.0, 60.0, 140.0])
+        fl._params_prev = None
+        fl._walls.prev_buf[:] = np.nan
+        fl.simFrame()
+        if fl.diffuse is not None:
             fl.diffuse.pollDebug()
-        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        else:
+            fl.sync()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    fl.destroy()
     h2d = 80 + 336 + 80
-    d2h = 4
+    d2h = 4 if scene.diffuse_max else 0
 
     n = scene.n
     total_updates = n * args.steps * ws
@@ -259,7 +271,6 @@ def main():
     e2e_value = total_updates / e2e_s
     peak, peak_src = measured_peaks()
     G = scene.cells
-    names = [lib.mpm_phase_name(i).decode() for i in range(10)]
     phase_ms = {names[i]: pm[i] / pc[i] for i in range(10) if pc[i]}
     dom = max((k for k in phase_ms if k in PHASE_BYTES), key=lambda k: phase_ms[k])
     bn, bg = PHASE_BYTES[dom]
@@ -298,7 +309,6 @@ def main():
                                 "sample": f"{done} substeps of {args.workload} ({secs:.1f} s) on {threads} threads"}
     if dist is not None:
         dist.barrier()
-    fl.destroy()
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

@@ -385,7 +385,7 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     if (d.enabled) return fail(MPM_ERR_BUSY, "diffuse already enabled");
     const size_t M = max_count, N = s.capacity;
     const size_t nwN = (N + 31) / 32, nwM = (M + 31) / 32;
-    const size_t nb = std::max((nwN + kRankThreads - 1) / kRankThreads, (nwM + kRankThreads - 1) / kRankThreads) + 1;
+    const size_t nb = std::max((N + kGroupIds - 1) / kGroupIds, (M + kGroupIds - 1) / kGroupIds) + 1;
     cudaError_t e = dalloc(&d.pool, M * 48);
     if (e == cudaSuccess) e = dalloc(&d.free_list, M * 4);
     if (e == cudaSuccess) e = dalloc(&d.top, 16);

@@ -2,17 +2,26 @@
 //
 // Same arithmetic as mpm_kernels.cu (and so the same bits), organised for
 // the B200:
-//   * Particles live in cell-sorted order (double-buffered, SoA-ish):
-//       posm  float4 (x, y, z, mass)    velid float4 (vx, vy, vz, id bits)
-//       aff   9 floats                  dens  float
-//     G2P writes the next state in the current sorted order and counts each
-//     particle into its new cell; the next substep's binning turns the counts
-//     into cell ranges and a permutation (sorted slot -> previous slot).
-//   * Work item = up to `chunk` particles of one cell.  One thread owns an
+//   * Work item = up to kMaxL particles of one cell.  One thread owns an
 //     item: the 27 neighbour masses (P2G_MOM) or velocities (G2P) are loaded
 //     once per item, and P2G contributions are summed in registers as i32
-//     (the same wrapping sums the reference's atomics produce) and flushed
-//     with one atomic per (cell, component) per item.
+//     (the same wrapping sums the reference's atomics produce), flushed with
+//     one atomic per (cell, component) per item.
+//   * Items are bucketed by length, and particles are stored warp-interleaved:
+//     the k-th particle of the item held by lane l of warp w of bucket b sits
+//     at position pos_off[b] + w*32*b + k*32 + l.  All 32 lanes of a warp run
+//     the same trip count and every per-particle load/store is coalesced.
+//   * Within a bucket, items are ordered by (tile, cell) — a deterministic
+//     layout that changes little from one substep to the next, so reading a
+//     particle through the permutation (new position -> previous position)
+//     stays nearly coalesced.  Cells holding more than kMaxL particles are
+//     split into several items placed after the ordered ones.
+//   * State (double-buffered, indexed by position):
+//       posm  float4 (x, y, z, mass)    velid float4 (vx, vy, vz, id bits)
+//       aff   9 planes                  dens  float
+//     G2P writes the next state in the current layout and the binning cell
+//     of every particle; the next substep counts particles per cell, turns
+//     the counts into items and a permutation.
 //   * The grid is processed per tile (16x8x8 cells) and only for tiles a
 //     particle stencil touches now or touched last substep (cells elsewhere
 //     are zero, as the reference's CLEAR/DECODE/UPDATE would leave them).
@@ -47,106 +56,73 @@ __device__ __forceinline__ int32_t clampi(int32_t v, int32_t lo, int32_t hi) { r
 // Binning
 // ---------------------------------------------------------------------------
 
-// Count particle `j` of state buffer `cur` into its cell; mark the tiles its
-// 3x3x3 stencil touches.  Cells are clamped into the grid for binning only.
-__device__ __forceinline__ void bin_particle(const FastView& v, uint32_t j, float px, float py, float pz) {
-    int32_t cx, cy, cz;
-    float fx, fy, fz;
-    cell_frac(px, cx, fx);
-    cell_frac(py, cy, fy);
-    cell_frac(pz, cz, fz);
-    cx = clampi(cx, 0, (int32_t)v.X - 1);
-    cy = clampi(cy, 0, (int32_t)v.Y - 1);
-    cz = clampi(cz, 0, (int32_t)v.Z - 1);
-    const uint32_t c = cell_of(cx, cy, cz, v.X, v.Y);
-    const uint32_t r = atomicAdd(&v.cell_count[c], 1u);
-    v.key[j] = c;
-    v.rank[j] = r;
-    const int32_t tx0 = max(cx - 1, 0) / kTileX, tx1 = min(cx + 1, (int32_t)v.X - 1) / kTileX;
-    const int32_t ty0 = max(cy - 1, 0) / kTileY, ty1 = min(cy + 1, (int32_t)v.Y - 1) / kTileY;
-    const int32_t tz0 = max(cz - 1, 0) / kTileZ, tz1 = min(cz + 1, (int32_t)v.Z - 1) / kTileZ;
-    const uint32_t own = ((uint32_t)(cz / kTileZ) * v.nty + (uint32_t)(cy / kTileY)) * v.ntx + (uint32_t)(cx / kTileX);
-    if ((v.tile_flags[own] & 3u) != 3u) atomicOr(&v.tile_flags[own], 3u);   // occupied (bit0) + stencil (bit1)
-    if (tx0 != tx1 || ty0 != ty1 || tz0 != tz1) {
-        for (int32_t tz = tz0; tz <= tz1; ++tz)
-            for (int32_t ty = ty0; ty <= ty1; ++ty)
-                for (int32_t tx = tx0; tx <= tx1; ++tx) {
-                    const uint32_t t = ((uint32_t)tz * v.nty + (uint32_t)ty) * v.ntx + (uint32_t)tx;
-                    if (t != own) atomicOr(&v.tile_flags[t], 2u);
-                }
-    }
+__device__ __forceinline__ uint32_t tile_of(const FastView& v, int32_t cx, int32_t cy, int32_t cz) {
+    return ((uint32_t)(cz / kTileZ) * v.nty + (uint32_t)(cy / kTileY)) * v.ntx + (uint32_t)(cx / kTileX);
 }
 
-// Identity-order import: keys for the state just copied in.
+// Mark a tile as holding particles for the next substep (bit 0).
+__device__ __forceinline__ void mark_occupied(const FastView& v, uint32_t t) {
+    if ((v.tile_flags[t] & 1u) == 0u) atomicOr(&v.tile_flags[t], 1u);
+}
+
+// Binning cell of a position (clamped into the grid; binning only).
+__device__ __forceinline__ void bin_cell(const FastView& v, float px, float py, float pz, int32_t& cx, int32_t& cy,
+                                         int32_t& cz) {
+    cx = clampi(__float2int_rz(floorf(px)), 0, (int32_t)v.X - 1);
+    cy = clampi(__float2int_rz(floorf(py)), 0, (int32_t)v.Y - 1);
+    cz = clampi(__float2int_rz(floorf(pz)), 0, (int32_t)v.Z - 1);
+}
+
+// Identity-layout import: binning cells for the state just copied in.
 __global__ void k_import_keys(FastView v, const float4* __restrict__ posm, uint32_t n) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0) {
+        v.ctrl->total_pos = n;
+        v.ctrl->prev_total_pos = n;
+    }
     if (j >= n) return;
     const float4 q = posm[j];
-    bin_particle(v, j, q.x, q.y, q.z);
+    int32_t cx, cy, cz;
+    bin_cell(v, q.x, q.y, q.z, cx, cy, cz);
+    v.key[j] = cell_of(cx, cy, cz, v.X, v.Y);
+    mark_occupied(v, tile_of(v, cx, cy, cz));
 }
 
-// Per substep: build the occupied-tile list (for binning) and the grid-tile
-// list (stencil tiles of this substep or the last one, plus the hand box);
-// shift the flags.  tile_flags bits: 0 occupied, 1 stencil (this substep),
-// 2 stencil (last substep), 3 hand box (this substep).
-__global__ void k_tiles(FastView v, int32_t hx0, int32_t hy0, int32_t hz0, int32_t hx1, int32_t hy1, int32_t hz1) {
+// Rank of every particle of the current state within its binning cell.
+__global__ void k_count(FastView v) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= v.ctrl->total_pos) return;
+    const uint32_t c = v.key[i];
+    if (c != kHole) v.rank[i] = atomicAdd(&v.cell_count[c], 1u);
+}
+
+// Occupied-tile list for the binning and the occupancy used by the scans.
+// tile_flags bits: 0 occupied (set by G2P), 1 stencil now (set by the
+// binning), 2 stencil last substep.
+__global__ void k_tiles_occ(FastView v) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= v.ntiles) return;
-    uint32_t f = v.tile_flags[t];
-    const uint32_t tx = t % v.ntx, ty = (t / v.ntx) % v.nty, tz = t / (v.ntx * v.nty);
-    if (hx0 <= hx1) {
-        const int32_t x0 = (int32_t)tx * kTileX, y0 = (int32_t)ty * kTileY, z0 = (int32_t)tz * kTileZ;
-        if (x0 <= hx1 && x0 + kTileX - 1 >= hx0 && y0 <= hy1 && y0 + kTileY - 1 >= hy0 && z0 <= hz1 &&
-            z0 + kTileZ - 1 >= hz0)
-            f |= 8u;
-    }
-    const bool occ = f & 1u;
-    const bool now = (f & (2u | 8u)) != 0;
-    const bool prev = (f & 4u) != 0;
-    if (occ) v.tile_occ_list[atomicAdd(&v.counters[kCntOcc], 1u)] = t;
-    if (now || prev) v.tile_grid_list[atomicAdd(&v.counters[kCntGrid], 1u)] = t;
-    v.tile_flags[t] = now ? 4u : 0u;
+    const uint32_t occ = v.tile_flags[t] & 1u;
+    v.tile_occ[t] = occ;
+    if (occ) v.tile_occ_list[atomicAdd(&v.ctrl->n_occ, 1u)] = t;
 }
 
-// Block-wide exclusive scan of one value per thread (blockDim.x == 1024).
-__device__ __forceinline__ uint32_t block_scan_1024(uint32_t x, uint32_t* total, uint32_t* ws) {
+// One block per occupied tile, one thread per cell.  A cell with 1..kMaxL
+// particles becomes one item in bucket `count`, ranked within the tile by
+// cell index (match + warp prefix); the tile's per-bucket totals go to
+// tile_hist.  Larger cells are split into items that take unordered slots
+// after the ordered ones.  Also marks every tile the particles' 3x3x3
+// stencils touch (bit 1) and clears the counts.
+__global__ void __launch_bounds__(kTileCells) k_bin_cells(FastView v) {
+    __shared__ uint32_t wcnt[kTileCells / 32][kMaxL + 1];
+    __shared__ uint32_t dirs;
+    const uint32_t nocc = v.ctrl->n_occ;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t s = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-        if (lane >= o) s += y;
-    }
-    if (lane == 31) ws[wid] = s;
-    __syncthreads();
-    if (wid == 0) {
-        uint32_t w = ws[lane];
-        uint32_t ww = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, ww, o);
-            if (lane >= o) ww += y;
-        }
-        ws[lane] = ww - w;   // exclusive warp offsets
-        if (lane == 31) ws[32] = ww;
-    }
-    __syncthreads();
-    const uint32_t r = ws[wid] + s - x;
-    *total = ws[32];
-    __syncthreads();
-    return r;
-}
-
-// One block per occupied tile (grid-stride over the list): cell counts ->
-// cell ranges in sorted order and work items (cell, begin, len <= chunk).
-__global__ void __launch_bounds__(kTileCells) k_bin_tiles(FastView v, uint32_t chunk) {
-    __shared__ uint32_t ws[33];
-    __shared__ uint32_t base_s[2];
-    const uint32_t nocc = v.counters[kCntOcc];
     for (uint32_t ti = blockIdx.x; ti < nocc; ti += gridDim.x) {
         const uint32_t t = v.tile_occ_list[ti];
         const uint32_t tx = t % v.ntx, ty = (t / v.ntx) % v.nty, tz = t / (v.ntx * v.nty);
-        const uint32_t lx = threadIdx.x % kTileX, ly = (threadIdx.x / kTileX) % kTileY, lz = threadIdx.x / (kTileX * kTileY);
+        const uint32_t lx = threadIdx.x % kTileX, ly = (threadIdx.x / kTileX) % kTileY,
+                       lz = threadIdx.x / (kTileX * kTileY);
         const uint32_t x = tx * kTileX + lx, y = ty * kTileY + ly, z = tz * kTileZ + lz;
         const bool inside = x < v.X && y < v.Y && z < v.Z;
         const uint32_t c = inside ? cell_of(x, y, z, v.X, v.Y) : 0u;
@@ -155,34 +131,220 @@ __global__ void __launch_bounds__(kTileCells) k_bin_tiles(FastView v, uint32_t c
             cnt = v.cell_count[c];
             if (cnt) v.cell_count[c] = 0u;
         }
-        const uint32_t nit = (cnt + chunk - 1) / chunk;
-        uint32_t tot, itot;
-        const uint32_t off = block_scan_1024(cnt, &tot, ws);
-        const uint32_t ioff = block_scan_1024(nit, &itot, ws);
-        if (threadIdx.x == 0) {
-            base_s[0] = tot ? atomicAdd(&v.counters[kCntSorted], tot) : 0u;
-            base_s[1] = itot ? atomicAdd(&v.counters[kCntItems], itot) : 0u;
+        if (threadIdx.x == 0) dirs = 0u;
+        for (int b = lane; b <= kMaxL; b += 32) wcnt[wid][b] = 0u;
+        __syncthreads();
+        // neighbour tiles this cell's stencil reaches (3x3x3 direction bits)
+        uint32_t m = 0;
+        if (cnt) {
+            const int dx = lx == 0 ? -1 : (lx == kTileX - 1 ? 1 : 0);
+            const int dy = ly == 0 ? -1 : (ly == kTileY - 1 ? 1 : 0);
+            const int dz = lz == 0 ? -1 : (lz == kTileZ - 1 ? 1 : 0);
+            for (int kz = 0; kz <= (dz != 0); ++kz)
+                for (int ky = 0; ky <= (dy != 0); ++ky)
+                    for (int kx = 0; kx <= (dx != 0); ++kx)
+                        m |= 1u << ((kz * dz + 1) * 9 + (ky * dy + 1) * 3 + (kx * dx + 1));
+        }
+        const uint32_t wm = __reduce_or_sync(0xffffffffu, m);
+        if (lane == 0 && wm) atomicOr(&dirs, wm);
+        const uint32_t b = (cnt >= 1 && cnt <= (uint32_t)kMaxL) ? cnt : 0u;
+        const uint32_t grp = __match_any_sync(0xffffffffu, b);
+        const uint32_t lrank = __popc(grp & ((1u << lane) - 1u));
+        if (b && lrank == 0) wcnt[wid][b] = __popc(grp);
+        __syncthreads();
+        // exclusive prefix over the 32 warps for each length; tile totals
+        if (threadIdx.x >= 1 && threadIdx.x <= kMaxL) {
+            uint32_t acc = 0;
+            for (int w = 0; w < kTileCells / 32; ++w) {
+                const uint32_t k = wcnt[w][threadIdx.x];
+                wcnt[w][threadIdx.x] = acc;
+                acc += k;
+            }
+            v.tile_hist[(threadIdx.x - 1) * v.ntiles + t] = acc;
+        }
+        if (threadIdx.x < 27 && ((dirs >> threadIdx.x) & 1u)) {
+            const int ox = (int)(threadIdx.x % 3) - 1, oy = (int)((threadIdx.x / 3) % 3) - 1,
+                      oz = (int)(threadIdx.x / 9) - 1;
+            const int nx = (int)tx + ox, ny = (int)ty + oy, nz = (int)tz + oz;
+            if (nx >= 0 && ny >= 0 && nz >= 0 && nx < (int)v.ntx && ny < (int)v.nty && nz < (int)v.ntz) {
+                const uint32_t nt = ((uint32_t)nz * v.nty + (uint32_t)ny) * v.ntx + (uint32_t)nx;
+                if ((v.tile_flags[nt] & 2u) == 0u) atomicOr(&v.tile_flags[nt], 2u);
+            }
         }
         __syncthreads();
-        if (cnt) {
-            const uint32_t b = base_s[0] + off;
-            v.cell_start[c] = b;
-            for (uint32_t k = 0; k < nit; ++k) {
-                const uint32_t beg = b + k * chunk;
-                const uint32_t len = min(chunk, cnt - k * chunk);
-                v.items[base_s[1] + ioff + k] = make_uint4(c, beg, len, 0u);
-            }
+        if (b) {
+            v.cell_info[c] = make_uint4(b | (b << 8) | (1u << 16), wcnt[wid][b] + lrank, 0u, 0u);
+        } else if (cnt) {
+            // overpacked cell: q items of length L (the last of Llast), unordered tail slots
+            const uint32_t q = (cnt + kMaxL - 1) / kMaxL;
+            const uint32_t L = (cnt + q - 1) / q;
+            const uint32_t Llast = cnt - (q - 1) * L;
+            const uint32_t nL = (Llast == L) ? q : q - 1;
+            const uint32_t idxL = atomicAdd(&v.ctrl->tail_cnt[L], nL);
+            const uint32_t idxLast = (Llast != L) ? atomicAdd(&v.ctrl->tail_cnt[Llast], 1u) : idxL + q - 1;
+            v.cell_info[c] = make_uint4(L | (Llast << 8) | (q << 16) | 0x80000000u, idxL, idxLast, 0u);
         }
         __syncthreads();
     }
 }
 
-// perm[sorted position] = previous slot
-__global__ void k_scatter(FastView v, uint32_t n) {
+// Grid-tile list (stencil tiles of this substep or the last one, plus the
+// hand box); shifts the flags for the next substep.
+__global__ void k_tiles_grid(FastView v, int32_t hx0, int32_t hy0, int32_t hz0, int32_t hx1, int32_t hy1,
+                             int32_t hz1) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= v.ntiles) return;
+    const uint32_t f = v.tile_flags[t];
+    const uint32_t tx = t % v.ntx, ty = (t / v.ntx) % v.nty, tz = t / (v.ntx * v.nty);
+    bool hand = false;
+    if (hx0 <= hx1) {
+        const int32_t x0 = (int32_t)tx * kTileX, y0 = (int32_t)ty * kTileY, z0 = (int32_t)tz * kTileZ;
+        hand = x0 <= hx1 && x0 + kTileX - 1 >= hx0 && y0 <= hy1 && y0 + kTileY - 1 >= hy0 && z0 <= hz1 &&
+               z0 + kTileZ - 1 >= hz0;
+    }
+    const bool now = (f & 2u) != 0 || hand || (v.tile_occ[t] != 0u);
+    const bool prev = (f & 4u) != 0;
+    if (now || prev) v.tile_grid_list[atomicAdd(&v.ctrl->n_grid, 1u)] = t;
+    if (f != (now ? 4u : 0u)) v.tile_flags[t] = now ? 4u : 0u;
+}
+
+// Per length bucket (one block each): exclusive scan of the ordered item
+// counts over all tiles in index order -> tile_base; total -> bucket_reg.
+__global__ void __launch_bounds__(1024) k_tile_scan(FastView v) {
+    __shared__ uint32_t ws[33];
+    const uint32_t b = blockIdx.x + 1;
+    const uint32_t* hist = v.tile_hist + (size_t)blockIdx.x * v.ntiles;
+    uint32_t* base = v.tile_base + (size_t)blockIdx.x * v.ntiles;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t carry = 0;
+    for (uint32_t t0 = 0; t0 < v.ntiles; t0 += 1024) {
+        const uint32_t t = t0 + threadIdx.x;
+        const uint32_t x = (t < v.ntiles && v.tile_occ[t]) ? hist[t] : 0u;
+        uint32_t sc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, sc, o);
+            if (lane >= o) sc += y;
+        }
+        if (lane == 31) ws[wid] = sc;
+        __syncthreads();
+        if (wid == 0) {
+            const uint32_t w = ws[lane];
+            uint32_t ww = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, ww, o);
+                if (lane >= o) ww += y;
+            }
+            ws[lane] = ww - w;
+            if (lane == 31) ws[32] = ww;
+        }
+        __syncthreads();
+        if (t < v.ntiles) base[t] = carry + ws[wid] + sc - x;
+        carry += ws[32];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) v.ctrl->bucket_reg[b] = carry;
+}
+
+// Bucket offsets (one warp): ordered + tail items, padded to whole warps.
+__global__ void k_bucket_scan(Ctrl* ctrl) {
+    const int lane = threadIdx.x;
+    const uint32_t b = (uint32_t)lane;
+    const uint32_t cnt = (b >= 1 && b <= (uint32_t)kMaxL) ? ctrl->bucket_reg[b] + ctrl->tail_cnt[b] : 0u;
+    const uint32_t pad = (cnt + 31u) & ~31u;
+    uint32_t si = pad, sp = pad * b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t yi = __shfl_up_sync(0xffffffffu, si, o);
+        const uint32_t yp = __shfl_up_sync(0xffffffffu, sp, o);
+        if (lane >= o) { si += yi; sp += yp; }
+    }
+    if (b <= (uint32_t)kMaxL + 1) {
+        ctrl->item_off[b] = si - pad;
+        ctrl->pos_off[b] = sp - pad * b;
+        ctrl->bucket_cnt[b] = cnt;
+    }
+    const uint32_t ti = __shfl_sync(0xffffffffu, si, kMaxL);
+    const uint32_t tp = __shfl_sync(0xffffffffu, sp, kMaxL);
+    if (lane == 0) {
+        ctrl->total_items = ti;
+        ctrl->prev_total_pos = ctrl->total_pos;
+        ctrl->total_pos = tp;
+    }
+}
+
+__device__ __forceinline__ uint32_t item_position(const uint32_t* pos_off, uint32_t b, uint32_t idx) {
+    return pos_off[b] + (idx >> 5) * 32u * b + (idx & 31u);
+}
+
+// perm[new position] = previous position for every particle; the first
+// particle of each item also records the item's cell.
+__global__ void k_scatter(FastView v) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t j = v.cell_start[v.key[i]] + v.rank[i];
-    if (j < n) v.perm[j] = i;
+    __shared__ uint32_t pos_off[kMaxL + 2];
+    __shared__ uint32_t reg[kMaxL + 2];
+    if (threadIdx.x < kMaxL + 2) {
+        pos_off[threadIdx.x] = v.ctrl->pos_off[threadIdx.x];
+        reg[threadIdx.x] = v.ctrl->bucket_reg[threadIdx.x];
+    }
+    __syncthreads();
+    if (i >= v.ctrl->prev_total_pos) return;
+    const uint32_t c = v.key[i];
+    if (c == kHole) return;
+    const uint32_t r = v.rank[i];
+    const uint4 info = v.cell_info[c];
+    uint32_t b, idx, kk;
+    if (!(info.x & 0x80000000u)) {
+        b = info.x & 0xFFu;
+        const int32_t cx = (int32_t)(c % v.X), cy = (int32_t)((c / v.X) % v.Y), cz = (int32_t)(c / (v.X * v.Y));
+        idx = v.tile_base[(b - 1) * v.ntiles + tile_of(v, cx, cy, cz)] + info.y;
+        kk = r;
+    } else {
+        const uint32_t L = info.x & 0xFFu, Llast = (info.x >> 8) & 0xFFu, q = (info.x >> 16) & 0x7FFFu;
+        const uint32_t it = r / L;
+        kk = r - it * L;
+        if (it + 1 < q || Llast == L) { b = L; idx = reg[L] + info.y + it; }
+        else { b = Llast; idx = reg[Llast] + info.z; }
+    }
+    if (b < 1 || b > (uint32_t)kMaxL) return;
+    const uint32_t pos = item_position(pos_off, b, idx) + kk * 32u;
+    if (pos >= v.npos) return;
+    v.perm[pos] = i;
+    if (kk == 0 && v.cap_off[b] + idx < v.cap_off[b + 1]) v.bucket_items[v.cap_off[b] + idx] = c;
+}
+
+// Shared copy of the bucket tables for the item kernels.
+struct ItemTables {
+    uint32_t item_off[kMaxL + 2];
+    uint32_t pos_off[kMaxL + 2];
+    uint32_t cnt[kMaxL + 2];
+};
+
+__device__ __forceinline__ void load_tables(const FastView& v, ItemTables& t) {
+    if (threadIdx.x < kMaxL + 2) {
+        t.item_off[threadIdx.x] = v.ctrl->item_off[threadIdx.x];
+        t.pos_off[threadIdx.x] = v.ctrl->pos_off[threadIdx.x];
+        t.cnt[threadIdx.x] = (threadIdx.x >= 1 && threadIdx.x <= kMaxL) ? v.ctrl->bucket_cnt[threadIdx.x] : 0u;
+    }
+    __syncthreads();
+}
+
+struct ItemRef {
+    uint32_t b, idx, cell, pbase;
+    bool valid;
+};
+
+__device__ __forceinline__ ItemRef item_ref(const FastView& v, const ItemTables& t, uint32_t g) {
+    ItemRef r;
+    uint32_t b = 1;
+    while (b < (uint32_t)kMaxL && g >= t.item_off[b + 1]) ++b;
+    r.b = b;
+    r.idx = g - t.item_off[b];
+    r.valid = r.idx < t.cnt[b];
+    r.cell = r.valid ? v.bucket_items[v.cap_off[b] + r.idx] : 0u;
+    r.pbase = item_position(t.pos_off, b, r.idx);
+    return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -205,46 +367,56 @@ __device__ __forceinline__ PW particle_weights(float px, float py, float pz) {
     return w;
 }
 
-__device__ __forceinline__ void item_cell(const FastView& v, uint32_t c, int32_t& x, int32_t& y, int32_t& z) {
+__device__ __forceinline__ void cell_xyz(const FastView& v, uint32_t c, int32_t& x, int32_t& y, int32_t& z) {
     x = (int32_t)(c % v.X);
     y = (int32_t)((c / v.X) % v.Y);
     z = (int32_t)(c / (v.X * v.Y));
 }
+
+// encode() without the clamp, for values already known to lie in +-20000.
+__device__ __forceinline__ int32_t encode_unclamped(float v) { return __float2int_rz(v * kFixed); }
 
 // ---------------------------------------------------------------------------
 // P2G_MASS (shaders.js:242-274), item-major
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kItemThreads) k_p2g_mass_items(FastView v, const float4* __restrict__ posm,
                                                                  int32_t* __restrict__ cm) {
-    const uint32_t nitems = v.counters[kCntItems];
+    __shared__ ItemTables tabs;
+    load_tables(v, tabs);
+    const uint32_t nitems = v.ctrl->total_items;
     const int32_t X = v.X, Y = v.Y, Z = v.Z;
-    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < nitems; it += gridDim.x * blockDim.x) {
-        const uint4 item = v.items[it];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nitems; g += gridDim.x * blockDim.x) {
+        const ItemRef it = item_ref(v, tabs, g);
+        if (!it.valid) continue;
         int32_t ix, iy, iz;
-        item_cell(v, item.x, ix, iy, iz);
+        cell_xyz(v, it.cell, ix, iy, iz);
         int32_t acc[27];
 #pragma unroll
         for (int q = 0; q < 27; ++q) acc[q] = 0;
-        for (uint32_t k = 0; k < item.z; ++k) {
-            const float4 p = posm[v.perm[item.y + k]];
+        for (uint32_t k = 0; k < it.b; ++k) {
+            const float4 p = posm[v.perm[it.pbase + k * 32u]];
             const PW w = particle_weights(p.x, p.y, p.z);
+            // weight <= 0.4219: for |mass| < 47000 encode's clamp is the identity
+            const bool safe = fabsf(p.w) < 47000.0f;
             if (w.cx == ix && w.cy == iy && w.cz == iz) {
                 float wxy[9];
 #pragma unroll
                 for (int j = 0; j < 3; ++j)
 #pragma unroll
                     for (int i = 0; i < 3; ++i) wxy[j * 3 + i] = w.wx[i] * w.wy[j];
+                if (safe) {
 #pragma unroll
-                for (int kk = 0; kk < 3; ++kk)
+                    for (int kk = 0; kk < 3; ++kk)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j)
+                        for (int q = 0; q < 9; ++q) acc[kk * 9 + q] += encode_unclamped(wxy[q] * w.wz[kk] * p.w);
+                } else {
 #pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const float ww = wxy[j * 3 + i] * w.wz[kk];
-                            acc[kk * 9 + j * 3 + i] += encode(ww * p.w);
-                        }
+                    for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+                        for (int q = 0; q < 9; ++q) acc[kk * 9 + q] += encode(wxy[q] * w.wz[kk] * p.w);
+                }
             } else {
-                // particle outside its binning cell (positions outside the grid): per-particle path
+                // particle outside its item's cell (positions outside the grid): per-particle path
                 for (int kk = 0; kk < 3; ++kk)
                     for (int j = 0; j < 3; ++j)
                         for (int i = 0; i < 3; ++i) {
@@ -286,8 +458,7 @@ __device__ __forceinline__ bool tile_cell(const FastView& v, uint32_t t, uint32_
 
 __global__ void __launch_bounds__(256) k_decode_tiles(FastView v, const int32_t* __restrict__ cm,
                                                       float* __restrict__ cmf) {
-    const uint32_t ng = v.counters[kCntGrid];
-    const uint32_t total = ng * kTileCells;
+    const uint32_t total = v.ctrl->n_grid * kTileCells;
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
         uint32_t c;
         int32_t x, y, z;
@@ -299,8 +470,7 @@ __global__ void __launch_bounds__(256) k_update_tiles(FastView v, const int32_t*
                                                       const int32_t* __restrict__ mv, float* __restrict__ mvf,
                                                       int32_t* __restrict__ cm_next, int32_t* __restrict__ mv_next,
                                                       const mpm_params P, const mpm_wall_params W) {
-    const uint32_t ng = v.counters[kCntGrid];
-    const uint32_t total = ng * kTileCells;
+    const uint32_t total = v.ctrl->n_grid * kTileCells;
     const uint32_t nw = wall_count_of(W.count_pad[0]);
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
         uint32_t idx;
@@ -357,24 +527,15 @@ struct MomIn {
 };
 
 // The scatter part of P2G_MOM for one particle whose density is known.
-// Adds the 81 encoded contributions into acc (or, with direct != nullptr,
-// atomically into the grid at the particle's own stencil).
-template <bool kDirect>
-__device__ __forceinline__ void mom_scatter(const PW& w, const MomIn& in, float density, const mpm_params& P,
-                                            int32_t* acc, int32_t* mv, uint32_t baseIdx, uint32_t G) {
-    const float rest = P.rest_density;
-    const float vol = __fdiv_rn(in.m, fmaxf(density, rest * 0.15f));
-    float pressure = P.stiffness * (eos_pow(__fdiv_rn(density, rest), P.eos_power) - 1.0f);
-    const float pFloor = density > rest * kCohesionGate ? kCohesionPressure : 0.0f;
-    pressure = fmaxf(pressure, pFloor);
-    const float visc = P.viscosity;
-    const float s00 = -pressure + visc * (in.a00 + in.a00);
-    const float s11 = -pressure + visc * (in.a11 + in.a11);
-    const float s22 = -pressure + visc * (in.a22 + in.a22);
-    const float s01 = visc * (in.a01 + in.a10);
-    const float s02 = visc * (in.a02 + in.a20);
-    const float s12 = visc * (in.a12 + in.a21);
-    const float coef = -vol * 4.0f * P.dt;
+// kDirect: atomics straight into the grid at the particle's own stencil;
+// otherwise the 81 encoded contributions are added into acc.
+// kClamp: full encode; without it the caller has bounded every value inside
+// +-20000, where encode's clamp is the identity.
+template <bool kDirect, bool kClamp>
+__device__ __forceinline__ void mom_scatter(const PW& w, const MomIn& in, const float* s, float coef,
+                                            const mpm_params& P, int32_t* acc, int32_t* mv, uint32_t baseIdx,
+                                            uint32_t G) {
+    const float s00 = s[0], s11 = s[1], s22 = s[2], s01 = s[3], s02 = s[4], s12 = s[5];
     const float dxs[3] = {-w.fx - 1.0f, -w.fx, 1.0f - w.fx};
     const float dys[3] = {-w.fy - 1.0f, -w.fy, 1.0f - w.fy};
     const float dzs[3] = {-w.fz - 1.0f, -w.fz, 1.0f - w.fz};
@@ -395,9 +556,12 @@ __device__ __forceinline__ void mom_scatter(const PW& w, const MomIn& in, float 
                 const float fxf = coef * (s00 * dxi + s01 * dyj + s02 * dzk);
                 const float fyf = coef * (s01 * dxi + s11 * dyj + s12 * dzk);
                 const float fzf = coef * (s02 * dxi + s12 * dyj + s22 * dzk);
-                const int32_t ex = encode(ww * (in.m * (in.vx + Qx) + fxf));
-                const int32_t ey = encode(ww * (in.m * (in.vy + Qy) + fyf));
-                const int32_t ez = encode(ww * (in.m * (in.vz + Qz) + fzf));
+                const float vx = ww * (in.m * (in.vx + Qx) + fxf);
+                const float vy = ww * (in.m * (in.vy + Qy) + fyf);
+                const float vz = ww * (in.m * (in.vz + Qz) + fzf);
+                const int32_t ex = kClamp ? encode(vx) : encode_unclamped(vx);
+                const int32_t ey = kClamp ? encode(vy) : encode_unclamped(vy);
+                const int32_t ez = kClamp ? encode(vz) : encode_unclamped(vz);
                 if (kDirect) {
                     const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
                     if (cidx < G) {
@@ -422,13 +586,17 @@ __global__ void __launch_bounds__(kItemThreads) k_p2g_mom_items(FastView v, cons
                                                                 const float* __restrict__ cmf,
                                                                 int32_t* __restrict__ mv, float* __restrict__ dens,
                                                                 const mpm_params P) {
-    const uint32_t nitems = v.counters[kCntItems];
+    __shared__ ItemTables tabs;
+    load_tables(v, tabs);
+    const uint32_t nitems = v.ctrl->total_items;
     const uint32_t X = P.grid_X, SLICE = P.grid_X * P.grid_Y;
     const uint32_t G = (uint32_t)v.G;
-    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < nitems; it += gridDim.x * blockDim.x) {
-        const uint4 item = v.items[it];
+    const size_t plane = v.npos;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nitems; g += gridDim.x * blockDim.x) {
+        const ItemRef it = item_ref(v, tabs, g);
+        if (!it.valid) continue;
         int32_t ix, iy, iz;
-        item_cell(v, item.x, ix, iy, iz);
+        cell_xyz(v, it.cell, ix, iy, iz);
         const uint32_t ibase = (uint32_t)(((iz - 1) * (int32_t)v.Y + (iy - 1)) * (int32_t)X + (ix - 1));
         float m27[27];
 #pragma unroll
@@ -443,13 +611,15 @@ __global__ void __launch_bounds__(kItemThreads) k_p2g_mom_items(FastView v, cons
         int32_t acc[81];
 #pragma unroll
         for (int q = 0; q < 81; ++q) acc[q] = 0;
-        for (uint32_t kk = 0; kk < item.z; ++kk) {
-            const uint32_t j = item.y + kk;
-            const uint32_t slot = v.perm[j];
+        for (uint32_t kk = 0; kk < it.b; ++kk) {
+            const uint32_t pos = it.pbase + kk * 32u;
+            const uint32_t slot = v.perm[pos];
             const float4 p = posm[slot];
             const float4 vv = velid[slot];
-            const float* a = aff + 9ull * slot;
-            MomIn in{vv.x, vv.y, vv.z, p.w, a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]};
+            MomIn in{vv.x, vv.y, vv.z, p.w,
+                     aff[slot], aff[plane + slot], aff[2 * plane + slot],
+                     aff[3 * plane + slot], aff[4 * plane + slot], aff[5 * plane + slot],
+                     aff[6 * plane + slot], aff[7 * plane + slot], aff[8 * plane + slot]};
             const PW w = particle_weights(p.x, p.y, p.z);
             const bool same = (w.cx == ix && w.cy == iy && w.cz == iz);
             const uint32_t baseIdx = (uint32_t)(((w.cz - 1) * (int32_t)v.Y + (w.cy - 1)) * (int32_t)X + (w.cx - 1));
@@ -470,10 +640,39 @@ __global__ void __launch_bounds__(kItemThreads) k_p2g_mom_items(FastView v, cons
                             density += w.wx[i] * w.wy[jj] * w.wz[k] * cmass;
                         }
             }
-            dens[j] = density;
+            dens[pos] = density;
             if (density <= 1e-8f) continue;
-            if (same) mom_scatter<false>(w, in, density, P, acc, mv, baseIdx, G);
-            else mom_scatter<true>(w, in, density, P, acc, mv, baseIdx, G);
+            // stress (shaders.js:325-338)
+            const float rest = P.rest_density;
+            const float vol = __fdiv_rn(in.m, fmaxf(density, rest * 0.15f));
+            float pressure = P.stiffness * (eos_pow(__fdiv_rn(density, rest), P.eos_power) - 1.0f);
+            const float pFloor = density > rest * kCohesionGate ? kCohesionPressure : 0.0f;
+            pressure = fmaxf(pressure, pFloor);
+            const float visc = P.viscosity;
+            float s[6];
+            s[0] = -pressure + visc * (in.a00 + in.a00);
+            s[1] = -pressure + visc * (in.a11 + in.a11);
+            s[2] = -pressure + visc * (in.a22 + in.a22);
+            s[3] = visc * (in.a01 + in.a10);
+            s[4] = visc * (in.a02 + in.a20);
+            s[5] = visc * (in.a12 + in.a21);
+            const float coef = -vol * 4.0f * P.dt;
+            // |value| <= 0.4219 * (|m| (|v| + 1.5 |A row|_1) + |coef| 1.5 |S row|_1): when that bound
+            // is well inside +-20000 encode's clamp cannot change any value (NaN/Inf fail the test).
+            const float am = fabsf(in.m), ac = fabsf(coef);
+            const float bx = am * (fabsf(in.vx) + 1.5f * (fabsf(in.a00) + fabsf(in.a01) + fabsf(in.a02))) +
+                             ac * 1.5f * (fabsf(s[0]) + fabsf(s[3]) + fabsf(s[4]));
+            const float by = am * (fabsf(in.vy) + 1.5f * (fabsf(in.a10) + fabsf(in.a11) + fabsf(in.a12))) +
+                             ac * 1.5f * (fabsf(s[3]) + fabsf(s[1]) + fabsf(s[5]));
+            const float bz = am * (fabsf(in.vz) + 1.5f * (fabsf(in.a20) + fabsf(in.a21) + fabsf(in.a22))) +
+                             ac * 1.5f * (fabsf(s[4]) + fabsf(s[5]) + fabsf(s[2]));
+            const bool safe = fmaxf(bx, fmaxf(by, bz)) * 0.4222f < 19000.0f;
+            if (same) {
+                if (safe) mom_scatter<false, false>(w, in, s, coef, P, acc, mv, baseIdx, G);
+                else mom_scatter<false, true>(w, in, s, coef, P, acc, mv, baseIdx, G);
+            } else {
+                mom_scatter<true, true>(w, in, s, coef, P, acc, mv, baseIdx, G);
+            }
         }
 #pragma unroll
         for (int k = 0; k < 3; ++k)
@@ -554,9 +753,9 @@ __device__ __forceinline__ bool spawn_record(uint32_t id, float4 q, float4 v, fl
     return true;
 }
 
-// G2P for one particle given its gathered grid velocity / B matrix.
-__device__ __forceinline__ void g2p_finish(const float4 q, float gvx, float gvy, float gvz, const float* B,
-                                           const mpm_params& P, const mpm_wall_params& W, f3& np, f3& nv) {
+// G2P for one particle given its gathered grid velocity (shaders.js:636-700).
+__device__ __forceinline__ void g2p_finish(const float4 q, float gvx, float gvy, float gvz, const mpm_params& P,
+                                           const mpm_wall_params& W, f3& np, f3& nv) {
     const float dt = P.dt, lk = P.lookahead_k, ws = P.wall_stiffness;
     np = mk(q.x + dt * gvx, q.y + dt * gvy, q.z + dt * gvz);
     nv = mk(gvx, gvy, gvz);
@@ -608,13 +807,29 @@ __global__ void __launch_bounds__(kItemThreads) k_g2p_items(FastView v, const fl
                                                             float4* __restrict__ velid_out,
                                                             float* __restrict__ aff_out, const mpm_params P,
                                                             const mpm_wall_params W, DiffuseView dv) {
-    const uint32_t nitems = v.counters[kCntItems];
+    __shared__ ItemTables tabs;
+    load_tables(v, tabs);
+    const uint32_t nitems = v.ctrl->total_items;
     const uint32_t X = P.grid_X, SLICE = P.grid_X * P.grid_Y;
     const uint32_t G = (uint32_t)v.G;
-    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < nitems; it += gridDim.x * blockDim.x) {
-        const uint4 item = v.items[it];
+    const size_t plane = v.npos;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nitems; g += gridDim.x * blockDim.x) {
+        const ItemRef it = item_ref(v, tabs, g);
+        if (!it.valid) {
+            // padding lane: mark its positions as holes for the next binning and the export
+            for (uint32_t kk = 0; kk < it.b; ++kk) {
+                const uint32_t pos = it.pbase + kk * 32u;
+                if (pos < v.npos) {
+                    v.key[pos] = kHole;
+                    velid_out[pos] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(kHole));
+                }
+            }
+            continue;
+        }
         int32_t ix, iy, iz;
-        item_cell(v, item.x, ix, iy, iz);
+        cell_xyz(v, it.cell, ix, iy, iz);
+        const uint32_t item_tile = tile_of(v, ix, iy, iz);
+        mark_occupied(v, item_tile);
         const uint32_t ibase = (uint32_t)(((iz - 1) * (int32_t)v.Y + (iy - 1)) * (int32_t)X + (ix - 1));
         float cv[81];
 #pragma unroll
@@ -632,9 +847,9 @@ __global__ void __launch_bounds__(kItemThreads) k_g2p_items(FastView v, const fl
                         cv[q + 0] = 0.0f; cv[q + 1] = 0.0f; cv[q + 2] = 0.0f;
                     }
                 }
-        for (uint32_t kk = 0; kk < item.z; ++kk) {
-            const uint32_t j = item.y + kk;
-            const uint32_t slot = v.perm[j];
+        for (uint32_t kk = 0; kk < it.b; ++kk) {
+            const uint32_t pos = it.pbase + kk * 32u;
+            const uint32_t slot = v.perm[pos];
             const float4 q = posm[slot];
             const float4 vi = velid[slot];
             const PW w = particle_weights(q.x, q.y, q.z);
@@ -675,19 +890,26 @@ __global__ void __launch_bounds__(kItemThreads) k_g2p_items(FastView v, const fl
                     }
                 }
             }
-            float* a = aff_out + 9ull * j;
 #pragma unroll
-            for (int e = 0; e < 9; ++e) a[e] = B[e] * 4.0f;
+            for (int e = 0; e < 9; ++e) aff_out[e * plane + pos] = B[e] * 4.0f;
             f3 np, nv;
-            g2p_finish(q, gvx, gvy, gvz, B, P, W, np, nv);
-            posm_out[j] = make_float4(np.x, np.y, np.z, q.w);
-            velid_out[j] = make_float4(nv.x, nv.y, nv.z, vi.w);
-            bin_particle(v, j, np.x, np.y, np.z);
+            g2p_finish(q, gvx, gvy, gvz, P, W, np, nv);
+            posm_out[pos] = make_float4(np.x, np.y, np.z, q.w);
+            velid_out[pos] = make_float4(nv.x, nv.y, nv.z, vi.w);
+            // binning of the new position
+            int32_t cx, cy, cz;
+            bin_cell(v, np.x, np.y, np.z, cx, cy, cz);
+            const uint32_t c = cell_of(cx, cy, cz, v.X, v.Y);
+            v.key[pos] = c;
+            if (c != it.cell) {
+                const uint32_t t = tile_of(v, cx, cy, cz);
+                if (t != item_tile) mark_occupied(v, t);
+            }
             if (dv.enabled && __float_as_uint(vi.w) < v.n) {
                 const uint32_t id = __float_as_uint(vi.w);
                 mpm_diffuse_particle r;
                 if (spawn_record(id, make_float4(np.x, np.y, np.z, 0.0f), make_float4(nv.x, nv.y, nv.z, 0.0f), q.w,
-                                 v.dens[j], dv.cmf, P, dv.gen, r)) {
+                                 v.dens[pos], dv.cmf, P, dv.gen, r)) {
                     dv.staging[id] = r;
                     atomicOr(&dv.spawn_bits[id >> 5], 1u << (id & 31u));
                 }
@@ -697,35 +919,36 @@ __global__ void __launch_bounds__(kItemThreads) k_g2p_items(FastView v, const fl
 }
 
 // ---------------------------------------------------------------------------
-// Import / export between the internal sorted state and reference layouts.
+// Import / export between the internal state and reference layouts.
 // ---------------------------------------------------------------------------
 __global__ void k_import(const float4* __restrict__ pos, const float4* __restrict__ vel,
                          const float* __restrict__ aff, const float* __restrict__ mass, float4* __restrict__ posm,
-                         float4* __restrict__ velid, float* __restrict__ aff_out, uint32_t n) {
+                         float4* __restrict__ velid, float* __restrict__ aff_out, uint32_t n, size_t plane) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i], v = vel[i];
     posm[i] = make_float4(p.x, p.y, p.z, mass[i]);
     velid[i] = make_float4(v.x, v.y, v.z, __uint_as_float(i));
 #pragma unroll
-    for (int e = 0; e < 9; ++e) aff_out[9ull * i + e] = aff[9ull * i + e];
+    for (int e = 0; e < 9; ++e) aff_out[e * plane + i] = aff[9ull * i + e];
 }
 
-__global__ void k_export(const float4* __restrict__ posm, const float4* __restrict__ velid,
-                         const float* __restrict__ aff, const float* __restrict__ dens, float4* __restrict__ pos,
-                         float4* __restrict__ vel, float* __restrict__ aff_out, float* __restrict__ mass,
-                         float* __restrict__ dens_out, uint32_t n) {
+__global__ void k_export(const Ctrl* __restrict__ ctrl, const float4* __restrict__ posm,
+                         const float4* __restrict__ velid, const float* __restrict__ aff,
+                         const float* __restrict__ dens, float4* __restrict__ pos, float4* __restrict__ vel,
+                         float* __restrict__ aff_out, float* __restrict__ mass, float* __restrict__ dens_out,
+                         uint32_t n, size_t plane) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
+    if (j >= ctrl->total_pos || j >= plane) return;
     const float4 p = posm[j], v = velid[j];
     const uint32_t id = __float_as_uint(v.w);
-    if (id >= n) return;
+    if (id >= n) return;   // padding position
     pos[id] = make_float4(p.x, p.y, p.z, 0.0f);
     vel[id] = make_float4(v.x, v.y, v.z, 0.0f);
     mass[id] = p.w;
     if (dens_out) dens_out[id] = dens[j];
 #pragma unroll
-    for (int e = 0; e < 9; ++e) aff_out[9ull * id + e] = aff[9ull * j + e];
+    for (int e = 0; e < 9; ++e) aff_out[9ull * id + e] = aff[e * plane + j];
 }
 
 inline uint32_t cdiv(uint64_t a, uint32_t b) { return (uint32_t)((a + b - 1) / b); }
@@ -733,7 +956,7 @@ inline uint32_t cdiv(uint64_t a, uint32_t b) { return (uint32_t)((a + b - 1) / b
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Host launchers
+// Host side
 // ---------------------------------------------------------------------------
 cudaError_t fast_alloc(FastEngine& f, uint32_t X, uint32_t Y, uint32_t Z, uint32_t capacity, int device) {
     f.X = X; f.Y = Y; f.Z = Z;
@@ -741,33 +964,44 @@ cudaError_t fast_alloc(FastEngine& f, uint32_t X, uint32_t Y, uint32_t Z, uint32
     f.ntx = cdiv(X, kTileX); f.nty = cdiv(Y, kTileY); f.ntz = cdiv(Z, kTileZ);
     f.ntiles = f.ntx * f.nty * f.ntz;
     f.capacity = capacity;
-    const size_t N = capacity ? capacity : 1;
+    f.npos = capacity + kPosSlack;
+    uint32_t off = 0;
+    f.cap_off[0] = 0;
+    for (int b = 1; b <= kMaxL; ++b) {
+        f.cap_off[b] = off;
+        off += capacity / b + 1;
+    }
+    f.cap_off[kMaxL + 1] = off;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     f.item_blocks = (uint32_t)sms * 8;
     f.grid_blocks = (uint32_t)sms * 8;
     f.bin_blocks = (uint32_t)sms * 2;
+    const size_t P = f.npos;
     cudaError_t e = cudaSuccess;
     auto A = [&](auto** p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc((void**)p, bytes ? bytes : 16);
     };
     for (int b = 0; b < 2; ++b) {
-        A(&f.posm[b], N * 16);
-        A(&f.velid[b], N * 16);
-        A(&f.aff[b], N * 36);
+        A(&f.posm[b], P * 16);
+        A(&f.velid[b], P * 16);
+        A(&f.aff[b], P * 36);
         A(&f.grid_i32[b], f.G * 16);
     }
-    A(&f.dens, N * 4);
+    A(&f.dens, P * 4);
     A(&f.cell_count, (f.G + 1) * 4);
-    A(&f.cell_start, f.G * 4);
-    A(&f.key, N * 4);
-    A(&f.rank, N * 4);
-    A(&f.perm, N * 4);
-    A(&f.items, N * 16);
+    A(&f.cell_info, f.G * 16);
+    A(&f.bucket_items, (size_t)off * 4);
+    A(&f.key, P * 4);
+    A(&f.rank, P * 4);
+    A(&f.perm, P * 4);
     A(&f.tile_flags, f.ntiles * 4);
+    A(&f.tile_occ, f.ntiles * 4);
+    A(&f.tile_hist, (size_t)kMaxL * f.ntiles * 4);
+    A(&f.tile_base, (size_t)kMaxL * f.ntiles * 4);
     A(&f.tile_occ_list, f.ntiles * 4);
     A(&f.tile_grid_list, f.ntiles * 4);
-    A(&f.counters, 64);
+    A(&f.ctrl, sizeof(Ctrl));
     if (e != cudaSuccess) return e;
     f.cm_current = f.grid_i32[0];
     return cudaSuccess;
@@ -775,8 +1009,8 @@ cudaError_t fast_alloc(FastEngine& f, uint32_t X, uint32_t Y, uint32_t Z, uint32
 
 void fast_free(FastEngine& f) {
     void* ptrs[] = {f.posm[0], f.posm[1], f.velid[0], f.velid[1], f.aff[0], f.aff[1], f.grid_i32[0], f.grid_i32[1],
-                    f.dens, f.cell_count, f.cell_start, f.key, f.rank, f.perm, f.items, f.tile_flags,
-                    f.tile_occ_list, f.tile_grid_list, f.counters};
+                    f.dens, f.cell_count, f.cell_info, f.bucket_items, f.key, f.rank, f.perm, f.tile_flags, f.tile_occ, f.tile_hist, f.tile_base,
+                    f.tile_occ_list, f.tile_grid_list, f.ctrl};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     f = FastEngine();
@@ -784,21 +1018,23 @@ void fast_free(FastEngine& f) {
 
 cudaError_t fast_import(FastEngine& f, const float4* pos, const float4* vel, const float* aff, const float* mass,
                         uint32_t n, cudaStream_t st) {
+    f.n = n;
     FastView v = f.view();
     cudaError_t e = cudaMemsetAsync(f.cell_count, 0, (f.G + 1) * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(f.tile_flags, 0, f.ntiles * 4, st);
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) e = cudaMemsetAsync(f.grid_i32[b], 0, 16 * f.G, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(f.dens, 0, (size_t)(f.capacity ? f.capacity : 1) * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(f.dens, 0, (size_t)f.npos * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(f.ctrl, 0, sizeof(Ctrl), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(f.key, 0xFF, (size_t)f.npos * 4, st);
+    // every permutation entry always names a valid position, even if a bug left one unwritten
+    if (e == cudaSuccess) e = cudaMemsetAsync(f.perm, 0, (size_t)f.npos * 4, st);
     if (e != cudaSuccess) return e;
-    f.cur = 0;
     f.gbuf = 0;
-    f.n = n;
+    f.cur = 0;
     f.cm_current = f.grid_i32[0];
-    if (n) {
-        k_import<<<cdiv(n, 256), 256, 0, st>>>(pos, vel, aff, mass, f.posm[0], f.velid[0], f.aff[0], n);
-        k_import_keys<<<cdiv(n, 256), 256, 0, st>>>(v, f.posm[0], n);
-        f.launches += 2;
-    }
+    if (n) k_import<<<cdiv(n, 256), 256, 0, st>>>(pos, vel, aff, mass, f.posm[0], f.velid[0], f.aff[0], n, f.npos);
+    k_import_keys<<<cdiv(n ? n : 1, 256), 256, 0, st>>>(v, f.posm[0], n);   // also sets the layout size
+    f.launches += n ? 2 : 1;
     f.dens_valid = false;
     return cudaGetLastError();
 }
@@ -806,8 +1042,8 @@ cudaError_t fast_import(FastEngine& f, const float4* pos, const float4* vel, con
 cudaError_t fast_export(FastEngine& f, float4* pos, float4* vel, float* aff, float* mass, float* dens,
                         cudaStream_t st) {
     if (f.n == 0) return cudaSuccess;
-    k_export<<<cdiv(f.n, 256), 256, 0, st>>>(f.posm[f.cur], f.velid[f.cur], f.aff[f.cur], f.dens, pos, vel, aff,
-                                            mass, dens, f.n);
+    k_export<<<cdiv(f.npos, 256), 256, 0, st>>>(f.ctrl, f.posm[f.cur], f.velid[f.cur], f.aff[f.cur], f.dens, pos, vel,
+                                                aff, mass, dens, f.n, f.npos);
     f.launches++;
     return cudaGetLastError();
 }
@@ -828,22 +1064,25 @@ cudaError_t fast_substep(Scene& s) {
     const bool hand = s.hand_active && s.hand_dims[0] > 0 && s.hand_dims[1] > 0 && s.hand_dims[2] > 0 &&
                       s.hand.is_on != 0u;
     int32_t hx0 = 1, hy0 = 1, hz0 = 1, hx1 = 0, hy1 = 0, hz1 = 0;
-    if (hand) {   // cells APPLY_HAND may write (its dispatch box clipped to the grid)
+    if (hand) {   // cells APPLY_HAND may write (its dispatch box clipped to bbox_max)
         hx0 = s.hand.bbox_min_x; hy0 = s.hand.bbox_min_y; hz0 = s.hand.bbox_min_z;
-        hx1 = s.hand.bbox_min_x + (s.hand_dims[0] + 3) / 4 * 4 - 1;
-        hy1 = s.hand.bbox_min_y + (s.hand_dims[1] + 3) / 4 * 4 - 1;
-        hz1 = s.hand.bbox_min_z + (s.hand_dims[2] + 3) / 4 * 4 - 1;
-        hx1 = min(hx1, s.hand.bbox_max_x); hy1 = min(hy1, s.hand.bbox_max_y); hz1 = min(hz1, s.hand.bbox_max_z);
+        hx1 = min(s.hand.bbox_min_x + (s.hand_dims[0] + 3) / 4 * 4 - 1, s.hand.bbox_max_x);
+        hy1 = min(s.hand.bbox_min_y + (s.hand_dims[1] + 3) / 4 * 4 - 1, s.hand.bbox_max_y);
+        hz1 = min(s.hand.bbox_min_z + (s.hand_dims[2] + 3) / 4 * 4 - 1, s.hand.bbox_max_z);
     }
     cudaError_t e;
     {
         Phase ph(s, MPM_PHASE_SORT);
-        e = cudaMemsetAsync(f.counters, 0, 64, st);
+        e = cudaMemsetAsync(f.ctrl, 0, kCtrlZeroBytes, st);
         if (e != cudaSuccess) return e;
-        k_tiles<<<cdiv(f.ntiles, 256), 256, 0, st>>>(v, hx0, hy0, hz0, hx1, hy1, hz1);
-        k_bin_tiles<<<f.bin_blocks, kTileCells, 0, st>>>(v, f.chunk);
-        if (n) k_scatter<<<cdiv(n, 256), 256, 0, st>>>(v, n);
-        f.launches += n ? 3 : 2;
+        k_count<<<cdiv(f.npos, 256), 256, 0, st>>>(v);
+        k_tiles_occ<<<cdiv(f.ntiles, 256), 256, 0, st>>>(v);
+        k_bin_cells<<<f.bin_blocks, kTileCells, 0, st>>>(v);
+        k_tiles_grid<<<cdiv(f.ntiles, 256), 256, 0, st>>>(v, hx0, hy0, hz0, hx1, hy1, hz1);
+        k_tile_scan<<<kMaxL, 1024, 0, st>>>(v);
+        k_bucket_scan<<<1, 32, 0, st>>>(f.ctrl);
+        k_scatter<<<cdiv(f.npos, 256), 256, 0, st>>>(v);
+        f.launches += 7;
     }
     if (n) {
         Phase ph(s, MPM_PHASE_P2G_MASS);
@@ -882,8 +1121,10 @@ cudaError_t fast_substep(Scene& s) {
         dv.staging = d.staging;
         dv.spawn_bits = d.spawn_bits;
         dv.cmf = s.cmf;
-        e = cudaMemsetAsync(d.spawn_bits, 0, ((size_t)(n + 31) / 32) * 4, st);
-        if (e != cudaSuccess) return e;
+        if (n) {
+            e = cudaMemsetAsync(d.spawn_bits, 0, ((size_t)(n + 31) / 32) * 4, st);
+            if (e != cudaSuccess) return e;
+        }
     }
     if (n) {
         Phase ph(s, MPM_PHASE_G2P);

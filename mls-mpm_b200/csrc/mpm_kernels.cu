@@ -23,6 +23,8 @@ namespace mpm {
 
 constexpr int kThreads = 256;
 
+static inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+
 // ---------------------------------------------------------------------------
 // P2G_MASS (shaders.js:242-274), weights of COMPUTE_WEIGHTS (shaders.js:216-240)
 // recomputed in registers.
@@ -404,6 +406,8 @@ __device__ __forceinline__ bool diffuse_spawn_record(uint32_t id, float4 q, floa
     return true;
 }
 
+// Plain engine: spawn decision per particle; one 256-thread block covers one
+// rank group, so the group's spawn count is written here too.
 __global__ void __launch_bounds__(kThreads) k_diffuse_gen_eval(const float4* __restrict__ pos,
                                                                 const float4* __restrict__ vel,
                                                                 const float* __restrict__ mass,
@@ -411,7 +415,8 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_gen_eval(const float4* __r
                                                                 const float* __restrict__ cmf, const mpm_params P,
                                                                 const mpm_gen_params gen,
                                                                 mpm_diffuse_particle* __restrict__ staging,
-                                                                uint32_t* __restrict__ bits) {
+                                                                uint32_t* __restrict__ bits,
+                                                                uint32_t* __restrict__ counts) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     bool s = false;
     if (p < P.particle_num) {
@@ -420,24 +425,28 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_gen_eval(const float4* __r
         if (s) staging[p] = r;
     }
     const unsigned b = __ballot_sync(0xffffffffu, s);
-    if ((threadIdx.x & 31) == 0 && (p >> 5) < (P.particle_num + 31u) / 32u) bits[p >> 5] = b;
-}
-
-// popcount of each kRankThreads-word group of a bitmask.
-__global__ void __launch_bounds__(kRankThreads) k_bits_count(const uint32_t* __restrict__ bits, uint32_t nwords,
-                                                              uint32_t* __restrict__ counts) {
-    const uint32_t w = blockIdx.x * kRankThreads + threadIdx.x;
-    uint32_t c = w < nwords ? __popc(bits[w]) : 0u;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    __shared__ uint32_t ws[kRankThreads / 32];
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __shared__ uint32_t wc[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) {
+        if ((p >> 5) < (P.particle_num + 31u) / 32u) bits[p >> 5] = b;
+        wc[threadIdx.x >> 5] = __popc(b);
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t t = 0;
-        for (int i = 0; i < kRankThreads / 32; ++i) t += ws[i];
+        for (int i = 0; i < kThreads / 32; ++i) t += wc[i];
         counts[blockIdx.x] = t;
     }
+}
+
+// Popcount of each group of kGroupIds ids (8 words; one thread per word).
+__global__ void __launch_bounds__(256) k_group_counts(const uint32_t* __restrict__ bits, uint32_t nwords,
+                                                      uint32_t* __restrict__ counts) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c = w < nwords ? __popc(bits[w]) : 0u;
+    c += __shfl_xor_sync(0xffffffffu, c, 1);
+    c += __shfl_xor_sync(0xffffffffu, c, 2);
+    c += __shfl_xor_sync(0xffffffffu, c, 4);
+    if ((w & 7u) == 0u && w < nwords) counts[w >> 3] = c;
 }
 
 // Exclusive scan of the group counts (one block).  Applies the pass to the
@@ -493,46 +502,33 @@ __global__ void __launch_bounds__(1024) k_rank_scan(uint32_t* __restrict__ count
     }
 }
 
-// Rank of each set bit: group offset + exclusive popcount within the group.
-__device__ __forceinline__ uint32_t group_rank_base(uint32_t word, const uint32_t* __restrict__ counts) {
-    __shared__ uint32_t ws[kRankThreads / 32];
-    const uint32_t c = __popc(word);
-    uint32_t x = c;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) ws[wid] = x;
-    __syncthreads();
-    uint32_t before = 0;
-    for (int i = 0; i < wid; ++i) before += ws[i];
-    return counts[blockIdx.x] + before + x - c;
+// Rank of set bit `id` among the set bits (ascending id).
+__device__ __forceinline__ uint32_t bit_rank(const uint32_t* __restrict__ bits, uint32_t word, uint32_t id,
+                                             const uint32_t* __restrict__ group_offsets) {
+    const uint32_t w = id >> 5;
+    uint32_t r = group_offsets[id / kGroupIds] + __popc(word & ((1u << (id & 31u)) - 1u));
+    for (uint32_t k = w & ~7u; k < w; ++k) r += __popc(bits[k]);
+    return r;
 }
 
-__global__ void __launch_bounds__(kRankThreads) k_diffuse_gen_write(const uint32_t* __restrict__ bits,
-                                                                     uint32_t nwords,
-                                                                     const uint32_t* __restrict__ counts,
-                                                                     const int32_t* __restrict__ state,
-                                                                     const uint32_t* __restrict__ free_list,
-                                                                     const mpm_diffuse_particle* __restrict__ staging,
-                                                                     mpm_diffuse_particle* __restrict__ pool,
-                                                                     uint32_t M) {
-    const uint32_t w = blockIdx.x * kRankThreads + threadIdx.x;
-    uint32_t word = w < nwords ? bits[w] : 0u;
-    uint32_t r = group_rank_base(word, counts);
+// Spawner of rank r takes free_list[top-1-r] if r < applied (one thread per id).
+__global__ void __launch_bounds__(256) k_spawn_write(const uint32_t* __restrict__ bits, uint32_t n,
+                                                     const uint32_t* __restrict__ counts,
+                                                     const int32_t* __restrict__ state,
+                                                     const uint32_t* __restrict__ free_list,
+                                                     const mpm_diffuse_particle* __restrict__ staging,
+                                                     mpm_diffuse_particle* __restrict__ pool, uint32_t M) {
+    const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const uint32_t word = bits[id >> 5];
+    if (!((word >> (id & 31u)) & 1u)) return;
+    const uint32_t r = bit_rank(bits, word, id, counts);
     const int32_t t0 = state[0], applied = state[2];
-    while (word) {
-        const int b = __ffs(word) - 1;
-        word &= word - 1;
-        const int32_t fi = t0 - 1 - (int32_t)r;
-        // free-list state uploaded by a caller may be inconsistent: never index outside the pool
-        if ((int32_t)r < applied && fi >= 0 && (uint32_t)fi < M) {
-            const uint32_t slot = free_list[fi];
-            if (slot < M) pool[slot] = staging[w * 32u + (uint32_t)b];
-        }
-        ++r;
+    const int32_t fi = t0 - 1 - (int32_t)r;
+    // free-list state uploaded by a caller may be inconsistent: never index outside the pool
+    if ((int32_t)r < applied && fi >= 0 && (uint32_t)fi < M) {
+        const uint32_t slot = free_list[fi];
+        if (slot < M) pool[slot] = staging[id];
     }
 }
 
@@ -585,7 +581,8 @@ __device__ __forceinline__ void reflect_axis(float& p, float& v, float lo, float
 __global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particle* __restrict__ pool,
                                                               const float* __restrict__ mvf, const mpm_params P,
                                                               const mpm_advect_params adv, const mpm_wall_params W,
-                                                              uint32_t* __restrict__ kill_bits) {
+                                                              uint32_t* __restrict__ kill_bits,
+                                                              uint32_t* __restrict__ counts) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t M = adv.diffuse_max;
     bool kill = false;
@@ -648,32 +645,32 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particl
         }
     }
     const unsigned b = __ballot_sync(0xffffffffu, kill);
-    if ((threadIdx.x & 31) == 0 && (i >> 5) < (M + 31u) / 32u) kill_bits[i >> 5] = b;
-}
-
-__global__ void __launch_bounds__(kRankThreads) k_diffuse_kill_push(const uint32_t* __restrict__ bits,
-                                                                     uint32_t nwords,
-                                                                     const uint32_t* __restrict__ counts,
-                                                                     const int32_t* __restrict__ state,
-                                                                     uint32_t* __restrict__ free_list, uint32_t M) {
-    const uint32_t w = blockIdx.x * kRankThreads + threadIdx.x;
-    uint32_t word = w < nwords ? bits[w] : 0u;
-    uint32_t r = group_rank_base(word, counts);
-    const int32_t t0 = state[0];
-    while (word) {
-        const int b = __ffs(word) - 1;
-        word &= word - 1;
-        const int32_t fi = t0 + (int32_t)r;
-        if (fi >= 0 && (uint32_t)fi < M) free_list[fi] = w * 32u + (uint32_t)b;
-        ++r;
+    __shared__ uint32_t wc[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) {
+        if ((i >> 5) < (M + 31u) / 32u) kill_bits[i >> 5] = b;
+        wc[threadIdx.x >> 5] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int k = 0; k < kThreads / 32; ++k) t += wc[k];
+        counts[blockIdx.x] = t;
     }
 }
 
-// ---------------------------------------------------------------------------
-// Host-side launch sequence for one substep (fluid-gpu.js:663-682,
-// diffuse-gpu.js:148-166).
-// ---------------------------------------------------------------------------
-static inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+// Killed slot of rank r goes to free_list[top + r] (one thread per slot).
+__global__ void __launch_bounds__(256) k_kill_push(const uint32_t* __restrict__ bits, uint32_t M,
+                                                   const uint32_t* __restrict__ counts,
+                                                   const int32_t* __restrict__ state,
+                                                   uint32_t* __restrict__ free_list) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const uint32_t word = bits[i >> 5];
+    if (!((word >> (i & 31u)) & 1u)) return;
+    const uint32_t r = bit_rank(bits, word, i, counts);
+    const int32_t fi = state[0] + (int32_t)r;
+    if (fi >= 0 && (uint32_t)fi < M) free_list[fi] = i;
+}
 
 cudaError_t launch_apply_hand(Scene& s) {
     dim3 grid(blocks_for(s.hand_dims[0], 4), blocks_for(s.hand_dims[1], 4), blocks_for(s.hand_dims[2], 4));
@@ -685,45 +682,41 @@ cudaError_t launch_apply_hand(Scene& s) {
 // decision pass runs here (plain engine); the binned engine makes that
 // decision in its G2P epilogue and has already bumped the seed.
 cudaError_t launch_diffuse(Scene& s, bool eval) {
+    static_assert(kThreads == (int)kGroupIds, "one rank group per 256-thread block");
     cudaStream_t st = s.stream;
     const mpm_params& P = s.params;
     DiffuseState& d = s.diffuse;
     const uint32_t n = P.particle_num;
     const uint32_t nwords = (n + 31u) / 32u;
-    const uint32_t nb = blocks_for(nwords, kRankThreads);
-    if (eval) {
-        d.seed = d.seed + 1u;                 // diffuse-gpu.js:149
-        mpm_gen_params gen = d.gen;
-        gen.seed = d.seed;
-        if (n > 0) {
-            Phase ph(s, MPM_PHASE_DIFFUSE_GEN);
-            k_diffuse_gen_eval<<<blocks_for(nwords * 32u, kThreads), kThreads, 0, st>>>(
-                s.pos, s.vel, s.mass, s.dens, s.cmf, P, gen, d.staging, d.spawn_bits);
-            s.launches++;
-        }
-    }
+    const uint32_t ng = blocks_for(n, kGroupIds);
     if (n > 0) {
         Phase ph(s, MPM_PHASE_DIFFUSE_GEN);
-        k_bits_count<<<nb, kRankThreads, 0, st>>>(d.spawn_bits, nwords, d.block_counts);
-        k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, nb, d.top, d.rank_state, 0);
-        k_diffuse_gen_write<<<nb, kRankThreads, 0, st>>>(d.spawn_bits, nwords, d.block_counts, d.rank_state,
-                                                          d.free_list, d.staging, d.pool, d.max_count);
+        if (eval) {
+            d.seed = d.seed + 1u;                 // diffuse-gpu.js:149
+            mpm_gen_params gen = d.gen;
+            gen.seed = d.seed;
+            k_diffuse_gen_eval<<<ng, kThreads, 0, st>>>(s.pos, s.vel, s.mass, s.dens, s.cmf, P, gen, d.staging,
+                                                        d.spawn_bits, d.block_counts);
+        } else {
+            k_group_counts<<<blocks_for(nwords, 256), 256, 0, st>>>(d.spawn_bits, nwords, d.block_counts);
+        }
+        k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, ng, d.top, d.rank_state, 0);
+        k_spawn_write<<<ng, 256, 0, st>>>(d.spawn_bits, n, d.block_counts, d.rank_state, d.free_list, d.staging,
+                                          d.pool, d.max_count);
         s.launches += 3;
+    } else if (eval) {
+        d.seed = d.seed + 1u;
     }
     const uint32_t M = d.max_count;
-    const uint32_t mwords = (M + 31u) / 32u;
-    const uint32_t mb = blocks_for(mwords, kRankThreads);
+    const uint32_t mg = blocks_for(M, kGroupIds);
     mpm_advect_params adv = d.adv;
     adv.diffuse_max = M;
     {
         Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
-        k_diffuse_advect<<<blocks_for(mwords * 32u, kThreads), kThreads, 0, st>>>(d.pool, s.mvf, P, adv, s.walls,
-                                                                                   d.kill_bits);
-        k_bits_count<<<mb, kRankThreads, 0, st>>>(d.kill_bits, mwords, d.block_counts);
-        k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mb, d.top, d.rank_state, 1);
-        k_diffuse_kill_push<<<mb, kRankThreads, 0, st>>>(d.kill_bits, mwords, d.block_counts, d.rank_state,
-                                                          d.free_list, M);
-        s.launches += 4;
+        k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, P, adv, s.walls, d.kill_bits, d.block_counts);
+        k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mg, d.top, d.rank_state, 1);
+        k_kill_push<<<mg, 256, 0, st>>>(d.kill_bits, M, d.block_counts, d.rank_state, d.free_list);
+        s.launches += 3;
     }
     return cudaGetLastError();
 }

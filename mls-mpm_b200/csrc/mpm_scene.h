@@ -12,10 +12,10 @@
 
 namespace mpm {
 
-// Scratch sizes for the deterministic free-list ranking (bitmask + per-block
-// popcounts + one scan).  kBitsPerBlock ids are covered by one rank block.
-constexpr uint32_t kRankThreads = 256;                 // words per rank block
-constexpr uint32_t kBitsPerBlock = kRankThreads * 32;  // ids per rank block
+// Deterministic free-list ranking: one bit per particle id (spawns) or pool
+// slot (kills), popcounts per group of kGroupIds ids, one exclusive scan over
+// the groups, then each set bit's rank = group offset + popcount before it.
+constexpr uint32_t kGroupIds = 256;                 // ids per group (8 words, one 256-thread block)
 
 struct DiffuseState {
     bool enabled = false;
