@@ -46,6 +46,27 @@ namespace {
 
 constexpr int kItemThreads = 128;
 
+// Register-pressure strategies of the item kernels (compile-time; defaults
+// are the measured best).
+#ifndef MPM_MOM_LB
+#define MPM_MOM_LB 1
+#endif
+#ifndef MPM_MOM_M27_SMEM
+#define MPM_MOM_M27_SMEM 0
+#endif
+#ifndef MPM_MOM_ACC_SMEM
+#define MPM_MOM_ACC_SMEM 1
+#endif
+#ifndef MPM_MOM_KLOOP
+#define MPM_MOM_KLOOP 1
+#endif
+#ifndef MPM_G2P_LB
+#define MPM_G2P_LB 3
+#endif
+#ifndef MPM_G2P_CV_SMEM
+#define MPM_G2P_CV_SMEM 0
+#endif
+
 __device__ __forceinline__ uint32_t cell_of(int32_t x, int32_t y, int32_t z, uint32_t X, uint32_t Y) {
     return ((uint32_t)z * Y + (uint32_t)y) * X + (uint32_t)x;
 }
@@ -526,6 +547,10 @@ struct MomIn {
     float a00, a01, a02, a10, a11, a12, a20, a21, a22;
 };
 
+#if MPM_MOM_ACC_SMEM
+__shared__ int32_t g_sacc[81][kItemThreads];   // per-thread accumulator slots (experiment)
+#endif
+
 // The scatter part of P2G_MOM for one particle whose density is known.
 // kDirect: atomics straight into the grid at the particle's own stencil;
 // otherwise the 81 encoded contributions are added into acc.
@@ -540,9 +565,14 @@ __device__ __forceinline__ void mom_scatter(const PW& w, const MomIn& in, const 
     const float dys[3] = {-w.fy - 1.0f, -w.fy, 1.0f - w.fy};
     const float dzs[3] = {-w.fz - 1.0f, -w.fz, 1.0f - w.fz};
     const uint32_t X = P.grid_X, SLICE = P.grid_X * P.grid_Y;
+#if MPM_MOM_KLOOP && MPM_MOM_ACC_SMEM
+#pragma unroll 1
+#else
 #pragma unroll
+#endif
     for (int k = 0; k < 3; ++k) {
-        const float wzk = w.wz[k], dzk = dzs[k];
+        const float wzk = k == 0 ? w.wz[0] : (k == 1 ? w.wz[1] : w.wz[2]);
+        const float dzk = k == 0 ? dzs[0] : (k == 1 ? dzs[1] : dzs[2]);
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             const float wyzk = w.wy[j] * wzk, dyj = dys[j];
@@ -571,16 +601,23 @@ __device__ __forceinline__ void mom_scatter(const PW& w, const MomIn& in, const 
                     }
                 } else {
                     const int q = (k * 9 + j * 3 + i) * 3;
+#if MPM_MOM_ACC_SMEM
+                    (void)acc;
+                    atomicAdd(&g_sacc[q + 0][threadIdx.x], ex);
+                    atomicAdd(&g_sacc[q + 1][threadIdx.x], ey);
+                    atomicAdd(&g_sacc[q + 2][threadIdx.x], ez);
+#else
                     acc[q + 0] += ex;
                     acc[q + 1] += ey;
                     acc[q + 2] += ez;
+#endif
                 }
             }
         }
     }
 }
 
-__global__ void __launch_bounds__(kItemThreads) k_p2g_mom_items(FastView v, const float4* __restrict__ posm,
+__global__ void __launch_bounds__(kItemThreads, MPM_MOM_LB) k_p2g_mom_items(FastView v, const float4* __restrict__ posm,
                                                                 const float4* __restrict__ velid,
                                                                 const float* __restrict__ aff,
                                                                 const float* __restrict__ cmf,
@@ -598,7 +635,13 @@ __global__ void __launch_bounds__(kItemThreads) k_p2g_mom_items(FastView v, cons
         int32_t ix, iy, iz;
         cell_xyz(v, it.cell, ix, iy, iz);
         const uint32_t ibase = (uint32_t)(((iz - 1) * (int32_t)v.Y + (iy - 1)) * (int32_t)X + (ix - 1));
+#if MPM_MOM_M27_SMEM
+        __shared__ float sm27[27][kItemThreads];
+#define M27(q) sm27[q][threadIdx.x]
+#else
         float m27[27];
+#define M27(q) m27[q]
+#endif
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
@@ -606,20 +649,51 @@ __global__ void __launch_bounds__(kItemThreads) k_p2g_mom_items(FastView v, cons
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
                     const uint32_t cidx = ibase + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
-                    m27[k * 9 + j * 3 + i] = cidx < G ? cmf[cidx] : 0.0f;
+                    M27(k * 9 + j * 3 + i) = cidx < G ? cmf[cidx] : 0.0f;
                 }
+#if MPM_MOM_ACC_SMEM
+#pragma unroll
+        for (int q = 0; q < 81; ++q) g_sacc[q][threadIdx.x] = 0;
+        int32_t* acc = nullptr;
+#else
         int32_t acc[81];
 #pragma unroll
         for (int q = 0; q < 81; ++q) acc[q] = 0;
+#endif
+        // software pipeline: the next particle's permutation entry and record are
+        // loaded while the current one is processed
+        uint32_t slot_n = it.b > 1 ? v.perm[it.pbase + 32u] : 0u;
+        float4 p_c, v_c;
+        float a_c[9];
+        {
+            const uint32_t slot = v.perm[it.pbase];
+            p_c = posm[slot];
+            v_c = velid[slot];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) a_c[e] = aff[e * plane + slot];
+        }
         for (uint32_t kk = 0; kk < it.b; ++kk) {
             const uint32_t pos = it.pbase + kk * 32u;
-            const uint32_t slot = v.perm[pos];
-            const float4 p = posm[slot];
-            const float4 vv = velid[slot];
-            MomIn in{vv.x, vv.y, vv.z, p.w,
-                     aff[slot], aff[plane + slot], aff[2 * plane + slot],
-                     aff[3 * plane + slot], aff[4 * plane + slot], aff[5 * plane + slot],
-                     aff[6 * plane + slot], aff[7 * plane + slot], aff[8 * plane + slot]};
+            float4 p_n = p_c, v_n = v_c;
+            float a_n[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) a_n[e] = a_c[e];
+            uint32_t slot_nn = slot_n;
+            if (kk + 1 < it.b) {
+                p_n = posm[slot_n];
+                v_n = velid[slot_n];
+#pragma unroll
+                for (int e = 0; e < 9; ++e) a_n[e] = aff[e * plane + slot_n];
+                if (kk + 2 < it.b) slot_nn = v.perm[pos + 64u];
+            }
+            const float4 p = p_c;
+            const MomIn in{v_c.x, v_c.y, v_c.z, p.w, a_c[0], a_c[1], a_c[2], a_c[3], a_c[4], a_c[5],
+                           a_c[6], a_c[7], a_c[8]};
+            p_c = p_n;
+            v_c = v_n;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) a_c[e] = a_n[e];
+            slot_n = slot_nn;
             const PW w = particle_weights(p.x, p.y, p.z);
             const bool same = (w.cx == ix && w.cy == iy && w.cz == iz);
             const uint32_t baseIdx = (uint32_t)(((w.cz - 1) * (int32_t)v.Y + (w.cy - 1)) * (int32_t)X + (w.cx - 1));
@@ -630,7 +704,7 @@ __global__ void __launch_bounds__(kItemThreads) k_p2g_mom_items(FastView v, cons
 #pragma unroll
                     for (int jj = 0; jj < 3; ++jj)
 #pragma unroll
-                        for (int i = 0; i < 3; ++i) density += w.wx[i] * w.wy[jj] * w.wz[k] * m27[k * 9 + jj * 3 + i];
+                        for (int i = 0; i < 3; ++i) density += w.wx[i] * w.wy[jj] * w.wz[k] * M27(k * 9 + jj * 3 + i);
             } else {
                 for (int k = 0; k < 3; ++k)
                     for (int jj = 0; jj < 3; ++jj)
@@ -682,10 +756,16 @@ __global__ void __launch_bounds__(kItemThreads) k_p2g_mom_items(FastView v, cons
                 for (int i = 0; i < 3; ++i) {
                     const uint32_t cidx = ibase + (uint32_t)k * SLICE + (uint32_t)jj * X + (uint32_t)i;
                     const int q = (k * 9 + jj * 3 + i) * 3;
+#if MPM_MOM_ACC_SMEM
+                    const int32_t a0 = g_sacc[q + 0][threadIdx.x], a1 = g_sacc[q + 1][threadIdx.x],
+                                  a2 = g_sacc[q + 2][threadIdx.x];
+#else
+                    const int32_t a0 = acc[q + 0], a1 = acc[q + 1], a2 = acc[q + 2];
+#endif
                     if (cidx < G) {
-                        if (acc[q + 0]) atomicAdd(mv + 3ull * cidx + 0, acc[q + 0]);
-                        if (acc[q + 1]) atomicAdd(mv + 3ull * cidx + 1, acc[q + 1]);
-                        if (acc[q + 2]) atomicAdd(mv + 3ull * cidx + 2, acc[q + 2]);
+                        if (a0) atomicAdd(mv + 3ull * cidx + 0, a0);
+                        if (a1) atomicAdd(mv + 3ull * cidx + 1, a1);
+                        if (a2) atomicAdd(mv + 3ull * cidx + 2, a2);
                     }
                 }
     }
@@ -800,7 +880,51 @@ __device__ __forceinline__ void g2p_finish(const float4 q, float gvx, float gvy,
     if (np.z > P.hard_max_z) { np.z = P.hard_max_z; nv.z = 0.0f; }
 }
 
-__global__ void __launch_bounds__(kItemThreads) k_g2p_items(FastView v, const float4* __restrict__ posm,
+// G2P gather for a particle outside its item's cell (positions outside the
+// grid): the reference's linear stencil index with a bounds guard.
+__device__ __noinline__ void g2p_gather_direct(const PW& w, const float4 q, const float* __restrict__ mvf,
+                                               const mpm_params& P, uint32_t G, float& gvx, float& gvy, float& gvz,
+                                               float* B) {
+    const uint32_t X = P.grid_X, SLICE = P.grid_X * P.grid_Y;
+    const int32_t bx = w.cx - 1, by = w.cy - 1, bz = w.cz - 1;
+    const uint32_t baseIdx = (uint32_t)((bz * (int32_t)P.grid_Y + by) * (int32_t)X + bx);
+    for (int k = 0; k < 3; ++k) {
+        const float wzk = w.wz[k];
+        const float dzk = __int2float_rn(bz + k) - q.z + 0.5f;
+        for (int jj = 0; jj < 3; ++jj) {
+            const float wyzk = w.wy[jj] * wzk;
+            const float dyj = __int2float_rn(by + jj) - q.y + 0.5f;
+            for (int i = 0; i < 3; ++i) {
+                const float ww = w.wx[i] * wyzk;
+                const float dxi = __int2float_rn(bx + i) - q.x + 0.5f;
+                const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)jj * X + (uint32_t)i;
+                float cvx = 0.0f, cvy = 0.0f, cvz = 0.0f;
+                if (cidx < G) {
+                    const float* c = mvf + 3ull * cidx;
+                    cvx = c[0]; cvy = c[1]; cvz = c[2];
+                }
+                const float wvx = ww * cvx, wvy = ww * cvy, wvz = ww * cvz;
+                gvx += wvx; gvy += wvy; gvz += wvz;
+                B[0] += wvx * dxi; B[1] += wvx * dyj; B[2] += wvx * dzk;
+                B[3] += wvy * dxi; B[4] += wvy * dyj; B[5] += wvy * dzk;
+                B[6] += wvz * dxi; B[7] += wvz * dyj; B[8] += wvz * dzk;
+            }
+        }
+    }
+}
+
+// Spawn decision + staging, out of line (most particles fail the density test first).
+__device__ __noinline__ void spawn_eval(uint32_t id, f3 np, f3 nv, float m, float density,
+                                        const mpm_params& P, const DiffuseView& dv) {
+    mpm_diffuse_particle r;
+    if (spawn_record(id, make_float4(np.x, np.y, np.z, 0.0f), make_float4(nv.x, nv.y, nv.z, 0.0f), m, density, dv.cmf,
+                     P, dv.gen, r)) {
+        dv.staging[id] = r;
+        atomicOr(&dv.spawn_bits[id >> 5], 1u << (id & 31u));
+    }
+}
+
+__global__ void __launch_bounds__(kItemThreads, MPM_G2P_LB) k_g2p_items(FastView v, const float4* __restrict__ posm,
                                                             const float4* __restrict__ velid,
                                                             const float* __restrict__ mvf,
                                                             float4* __restrict__ posm_out,
@@ -831,7 +955,13 @@ __global__ void __launch_bounds__(kItemThreads) k_g2p_items(FastView v, const fl
         const uint32_t item_tile = tile_of(v, ix, iy, iz);
         mark_occupied(v, item_tile);
         const uint32_t ibase = (uint32_t)(((iz - 1) * (int32_t)v.Y + (iy - 1)) * (int32_t)X + (ix - 1));
+#if MPM_G2P_CV_SMEM
+        __shared__ float scv[81][kItemThreads];
+#define CV(q) scv[q][threadIdx.x]
+#else
         float cv[81];
+#define CV(q) cv[q]
+#endif
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
@@ -842,53 +972,61 @@ __global__ void __launch_bounds__(kItemThreads) k_g2p_items(FastView v, const fl
                     const int q = (k * 9 + j * 3 + i) * 3;
                     if (cidx < G) {
                         const float* c = mvf + 3ull * cidx;
-                        cv[q + 0] = c[0]; cv[q + 1] = c[1]; cv[q + 2] = c[2];
+                        CV(q + 0) = c[0]; CV(q + 1) = c[1]; CV(q + 2) = c[2];
                     } else {
-                        cv[q + 0] = 0.0f; cv[q + 1] = 0.0f; cv[q + 2] = 0.0f;
+                        CV(q + 0) = 0.0f; CV(q + 1) = 0.0f; CV(q + 2) = 0.0f;
                     }
                 }
+        uint32_t slot_n = it.b > 1 ? v.perm[it.pbase + 32u] : 0u;
+        float4 q_c, vi_c;
+        {
+            const uint32_t slot = v.perm[it.pbase];
+            q_c = posm[slot];
+            vi_c = velid[slot];
+        }
         for (uint32_t kk = 0; kk < it.b; ++kk) {
             const uint32_t pos = it.pbase + kk * 32u;
-            const uint32_t slot = v.perm[pos];
-            const float4 q = posm[slot];
-            const float4 vi = velid[slot];
+            float4 q_n = q_c, vi_n = vi_c;
+            uint32_t slot_nn = slot_n;
+            if (kk + 1 < it.b) {
+                q_n = posm[slot_n];
+                vi_n = velid[slot_n];
+                if (kk + 2 < it.b) slot_nn = v.perm[pos + 64u];
+            }
+            const float4 q = q_c;
+            const float4 vi = vi_c;
+            q_c = q_n;
+            vi_c = vi_n;
+            slot_n = slot_nn;
             const PW w = particle_weights(q.x, q.y, q.z);
             const bool same = (w.cx == ix && w.cy == iy && w.cz == iz);
-            const int32_t bx = w.cx - 1, by = w.cy - 1, bz = w.cz - 1;
-            const uint32_t baseIdx = (uint32_t)((bz * (int32_t)v.Y + by) * (int32_t)X + bx);
             float gvx = 0.0f, gvy = 0.0f, gvz = 0.0f;
             float B[9] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            if (same) {
+                const int32_t bx = w.cx - 1, by = w.cy - 1, bz = w.cz - 1;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float wzk = w.wz[k];
-                const float dzk = __int2float_rn(bz + k) - q.z + 0.5f;
+                for (int k = 0; k < 3; ++k) {
+                    const float wzk = w.wz[k];
+                    const float dzk = __int2float_rn(bz + k) - q.z + 0.5f;
 #pragma unroll
-                for (int jj = 0; jj < 3; ++jj) {
-                    const float wyzk = w.wy[jj] * wzk;
-                    const float dyj = __int2float_rn(by + jj) - q.y + 0.5f;
+                    for (int jj = 0; jj < 3; ++jj) {
+                        const float wyzk = w.wy[jj] * wzk;
+                        const float dyj = __int2float_rn(by + jj) - q.y + 0.5f;
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        const float ww = w.wx[i] * wyzk;
-                        const float dxi = __int2float_rn(bx + i) - q.x + 0.5f;
-                        float cvx, cvy, cvz;
-                        if (same) {
+                        for (int i = 0; i < 3; ++i) {
+                            const float ww = w.wx[i] * wyzk;
+                            const float dxi = __int2float_rn(bx + i) - q.x + 0.5f;
                             const int qq = (k * 9 + jj * 3 + i) * 3;
-                            cvx = cv[qq + 0]; cvy = cv[qq + 1]; cvz = cv[qq + 2];
-                        } else {
-                            const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)jj * X + (uint32_t)i;
-                            cvx = cvy = cvz = 0.0f;
-                            if (cidx < G) {
-                                const float* c = mvf + 3ull * cidx;
-                                cvx = c[0]; cvy = c[1]; cvz = c[2];
-                            }
+                            const float wvx = ww * CV(qq + 0), wvy = ww * CV(qq + 1), wvz = ww * CV(qq + 2);
+                            gvx += wvx; gvy += wvy; gvz += wvz;
+                            B[0] += wvx * dxi; B[1] += wvx * dyj; B[2] += wvx * dzk;
+                            B[3] += wvy * dxi; B[4] += wvy * dyj; B[5] += wvy * dzk;
+                            B[6] += wvz * dxi; B[7] += wvz * dyj; B[8] += wvz * dzk;
                         }
-                        const float wvx = ww * cvx, wvy = ww * cvy, wvz = ww * cvz;
-                        gvx += wvx; gvy += wvy; gvz += wvz;
-                        B[0] += wvx * dxi; B[1] += wvx * dyj; B[2] += wvx * dzk;
-                        B[3] += wvy * dxi; B[4] += wvy * dyj; B[5] += wvy * dzk;
-                        B[6] += wvz * dxi; B[7] += wvz * dyj; B[8] += wvz * dzk;
                     }
                 }
+            } else {
+                g2p_gather_direct(w, q, mvf, P, G, gvx, gvy, gvz, B);
             }
 #pragma unroll
             for (int e = 0; e < 9; ++e) aff_out[e * plane + pos] = B[e] * 4.0f;
@@ -906,13 +1044,10 @@ __global__ void __launch_bounds__(kItemThreads) k_g2p_items(FastView v, const fl
                 if (t != item_tile) mark_occupied(v, t);
             }
             if (dv.enabled && __float_as_uint(vi.w) < v.n) {
-                const uint32_t id = __float_as_uint(vi.w);
-                mpm_diffuse_particle r;
-                if (spawn_record(id, make_float4(np.x, np.y, np.z, 0.0f), make_float4(nv.x, nv.y, nv.z, 0.0f), q.w,
-                                 v.dens[pos], dv.cmf, P, dv.gen, r)) {
-                    dv.staging[id] = r;
-                    atomicOr(&dv.spawn_bits[id >> 5], 1u << (id & 31u));
-                }
+                const float density = v.dens[pos];
+                // spawn_record's first test (shaders.js:806), checked inline
+                if (density > 0.0f && density <= dv.gen.density_bubble_min)
+                    spawn_eval(__float_as_uint(vi.w), np, nv, q.w, density, P, dv);
             }
         }
     }
