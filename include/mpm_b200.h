@@ -164,6 +164,49 @@ mpm_status mpm_diffuse_alive_count(mpm_scene* scene, int32_t* alive);
  * work after a step. */
 mpm_status mpm_get_stream(mpm_scene* scene, void** stream);
 
+/* ---- particle editing: deleteNear / raycastFluid / spawnParticles ---- */
+
+/* FluidGPU.deleteNear + pollDelete (fluid-gpu.js:544-592): removes the active
+ * particles within `radius` of the line through `origin` along `dir` (the
+ * COMPACT pass, shaders.js:521-546), keeping the survivors in index order;
+ * the affine buffer is not compacted (shaders.js:516-520).  Waits for the
+ * stream and returns the new active count in *new_count. */
+mpm_status mpm_delete_near(mpm_scene* scene, const double origin[3], const double dir[3], double radius,
+                           uint32_t* new_count);
+
+/* FluidGPU.raycastFluid + pollRaycast (fluid-gpu.js:594-628): the smallest t
+ * > 0 along the ray among active particles within `radius` of it (the
+ * RAYCAST pass, shaders.js:563-576).  *hit = 0 when none; else *t_out = t
+ * and hit_pos = origin + t * dir (in double, as the JS side computes it).
+ * Waits for the stream. */
+mpm_status mpm_raycast_fluid(mpm_scene* scene, const double origin[3], const double dir[3], double radius,
+                             int* hit, float* t_out, double hit_pos[3]);
+
+/* The buffer writes of FluidGPU.spawnParticles (fluid-gpu.js:145-179):
+ * appends min(count, capacity - active) particles (pos4/vel4 vec4<f32>,
+ * mass f32; vel4 may be NULL for zero velocity) after the active ones and
+ * raises the active count; *appended gets the number written.  The sphere
+ * sampling stays on the host side. */
+mpm_status mpm_append_particles(mpm_scene* scene, const float* pos4, const float* vel4, const float* mass,
+                                uint32_t count, uint32_t* appended);
+
+/* The COMPACT pass over caller-owned device buffers (shaders.js:521-546 with
+ * bindings 0-8 as arguments): survivors of pos_in/vel_in/mass_in (n
+ * particles) go to the front of pos_out/vel_out/mass_out in index order and
+ * *count_dev (device memory) receives their number.  Enqueued on `stream`
+ * (a cudaStream_t on the current device; NULL = legacy default stream); the
+ * per-block scratch is a stream-ordered allocation freed on that stream.
+ * Inputs and outputs must not overlap. */
+mpm_status mpm_compact(const mpm_ray_params* del, uint32_t n, const float* pos_in, const float* vel_in,
+                       const float* mass_in, float* pos_out, float* vel_out, float* mass_out, uint32_t* count_dev,
+                       void* stream);
+
+/* The RAYCAST pass over a caller-owned device buffer (shaders.js:563-576):
+ * *hit_dev (device memory) = the smallest f32 bit pattern of t among hits,
+ * 0xFFFFFFFF when none (the sentinel is written by this call). */
+mpm_status mpm_raycast(const mpm_ray_params* ray, uint32_t n, const float* pos_in, uint32_t* hit_dev,
+                       void* stream);
+
 /* ---- tracing (no counterpart in the reference, whose only timers are
  * render-pass timestamps, fluid-renderer.js:34-41) ---- */
 

@@ -2,6 +2,7 @@
 // uniforms, stepping and buffer export.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -10,6 +11,7 @@
 #include <vector>
 
 #include "../../include/mpm_b200.h"
+#include "mpm_edit.h"
 #include "mpm_kernels.h"
 #include "mpm_scene.h"
 
@@ -104,10 +106,12 @@ static void free_scene(Scene& s) {
     fast_free(s.fast);
     void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
                     s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
-                    s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.rank_state, s.diffuse.staging};
+                    s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.rank_state, s.diffuse.staging,
+                    s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s.diffuse.host_top) cudaFreeHost(s.diffuse.host_top);
+    if (s.edit_host) cudaFreeHost(s.edit_host);
     if (s.stream) cudaStreamDestroy(s.stream);
 }
 
@@ -496,6 +500,131 @@ mpm_status mpm_diffuse_alive_count(mpm_scene* sc, int32_t* alive) {
 mpm_status mpm_get_stream(mpm_scene* sc, void** stream) {
     if (!sc || !stream) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     *stream = (void*)sc->s.stream;
+    return MPM_OK;
+}
+
+// fluid-gpu.js:547-550 / 597-600: the RayParams uniform (f32) from JS numbers.
+static mpm_ray_params pack_ray(const double o[3], const double d[3], double radius) {
+    mpm_ray_params r;
+    r.ox = (float)o[0]; r.oy = (float)o[1]; r.oz = (float)o[2];
+    r.radius = (float)radius;
+    r.dx = (float)d[0]; r.dy = (float)d[1]; r.dz = (float)d[2];
+    r._pad = 0.0f;
+    return r;
+}
+
+static cudaError_t ensure_edit_scratch(Scene& s, bool compact) {
+    cudaError_t e = cudaSuccess;
+    if (!s.edit_word) e = dalloc(&s.edit_word, 16);
+    if (e == cudaSuccess && !s.edit_host) e = cudaMallocHost((void**)&s.edit_host, 16);
+    if (!compact || e != cudaSuccess || s.edit_pos) return e;
+    const size_t N = s.capacity;
+    e = dalloc(&s.edit_pos, N * 16);
+    if (e == cudaSuccess) e = dalloc(&s.edit_vel, N * 16);
+    if (e == cudaSuccess) e = dalloc(&s.edit_mass, N * 4);
+    if (e == cudaSuccess) e = dalloc(&s.edit_blocks, compact_scratch_words(N) * 4);
+    if (e != cudaSuccess) {
+        cudaFree(s.edit_pos); cudaFree(s.edit_vel); cudaFree(s.edit_mass); cudaFree(s.edit_blocks);
+        s.edit_pos = nullptr; s.edit_vel = nullptr; s.edit_mass = nullptr; s.edit_blocks = nullptr;
+    }
+    return e;
+}
+
+mpm_status mpm_delete_near(mpm_scene* sc, const double origin[3], const double dir[3], double radius,
+                           uint32_t* new_count) {
+    if (!sc || !origin || !dir || !new_count) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    Scene& s = sc->s;
+    DeviceGuard guard(s.device);
+    CUDA_TRY(ensure_edit_scratch(s, true), "deleteNear scratch");
+    CUDA_TRY(sync_reference_buffers(s), "export");
+    const mpm_ray_params del = pack_ray(origin, dir, radius);
+    const uint32_t n = s.params.particle_num;
+    cudaStream_t st = s.stream;
+    CUDA_TRY(launch_compact(del, n, s.pos, s.vel, s.mass, s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks,
+                            s.edit_word, st),
+             "compact");
+    s.launches += n ? 3 : 0;
+    CUDA_TRY(cudaMemcpyAsync(s.edit_host, s.edit_word, 4, cudaMemcpyDeviceToHost, st), "count readback");
+    CUDA_TRY(cudaStreamSynchronize(st), "compact sync");
+    const uint32_t m = *s.edit_host;
+    // survivors back into the main buffers (fluid-gpu.js:566-568)
+    CUDA_TRY(cudaMemcpyAsync(s.pos, s.edit_pos, (size_t)m * 16, cudaMemcpyDeviceToDevice, st), "copy pos");
+    CUDA_TRY(cudaMemcpyAsync(s.vel, s.edit_vel, (size_t)m * 16, cudaMemcpyDeviceToDevice, st), "copy vel");
+    CUDA_TRY(cudaMemcpyAsync(s.mass, s.edit_mass, (size_t)m * 4, cudaMemcpyDeviceToDevice, st), "copy mass");
+    s.params.particle_num = m;
+    s.n_active = m;
+    if (s.engine == kEngineBinned) s.fast_stale = true;
+    *new_count = m;
+    return MPM_OK;
+}
+
+mpm_status mpm_raycast_fluid(mpm_scene* sc, const double origin[3], const double dir[3], double radius, int* hit,
+                             float* t_out, double hit_pos[3]) {
+    if (!sc || !origin || !dir || !hit) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    Scene& s = sc->s;
+    DeviceGuard guard(s.device);
+    CUDA_TRY(ensure_edit_scratch(s, false), "raycast scratch");
+    CUDA_TRY(sync_reference_buffers(s), "export");
+    const mpm_ray_params ray = pack_ray(origin, dir, radius);
+    CUDA_TRY(launch_raycast(ray, s.params.particle_num, s.pos, s.edit_word, s.stream), "raycast");
+    s.launches += s.params.particle_num ? 1 : 0;
+    CUDA_TRY(cudaMemcpyAsync(s.edit_host, s.edit_word, 4, cudaMemcpyDeviceToHost, s.stream), "hit readback");
+    CUDA_TRY(cudaStreamSynchronize(s.stream), "raycast sync");
+    const uint32_t bits = *s.edit_host;
+    // pollRaycast (fluid-gpu.js:617-627)
+    *hit = bits != 0xFFFFFFFFu;
+    if (*hit) {
+        float t;
+        std::memcpy(&t, &bits, 4);
+        if (t_out) *t_out = t;
+        if (hit_pos)
+            for (int i = 0; i < 3; ++i) hit_pos[i] = origin[i] + (double)t * dir[i];
+    }
+    return MPM_OK;
+}
+
+mpm_status mpm_append_particles(mpm_scene* sc, const float* pos4, const float* vel4, const float* mass,
+                                uint32_t count, uint32_t* appended) {
+    if (!sc || !appended || (count && (!pos4 || !mass))) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    Scene& s = sc->s;
+    const uint32_t start = s.params.particle_num;
+    const uint32_t n = std::min<uint32_t>(count, s.capacity - start);   // fluid-gpu.js:147-149
+    *appended = 0;
+    if (n == 0) return MPM_OK;
+    DeviceGuard guard(s.device);
+    cudaStream_t st = s.stream;
+    CUDA_TRY(sync_reference_buffers(s), "export");
+    CUDA_TRY(cudaMemcpyAsync(s.pos + start, pos4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "append pos");
+    if (vel4) CUDA_TRY(cudaMemcpyAsync(s.vel + start, vel4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "append vel");
+    else CUDA_TRY(cudaMemsetAsync(s.vel + start, 0, (size_t)n * 16, st), "append vel");
+    CUDA_TRY(cudaMemcpyAsync(s.mass + start, mass, (size_t)n * 4, cudaMemcpyHostToDevice, st), "append mass");
+    CUDA_TRY(cudaStreamSynchronize(st), "append sync");
+    s.params.particle_num = start + n;
+    s.n_active = start + n;
+    if (s.engine == kEngineBinned) s.fast_stale = true;
+    *appended = n;
+    return MPM_OK;
+}
+
+mpm_status mpm_compact(const mpm_ray_params* del, uint32_t n, const float* pos_in, const float* vel_in,
+                       const float* mass_in, float* pos_out, float* vel_out, float* mass_out, uint32_t* count_dev,
+                       void* stream) {
+    if (!del || !count_dev || (n && (!pos_in || !vel_in || !mass_in || !pos_out || !vel_out || !mass_out)))
+        return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t* scratch = nullptr;
+    CUDA_TRY(cudaMallocAsync((void**)&scratch, compact_scratch_words(n) * 4, st), "compact scratch");
+    const cudaError_t e = launch_compact(*del, n, (const float4*)pos_in, (const float4*)vel_in, mass_in,
+                                         (float4*)pos_out, (float4*)vel_out, mass_out, scratch, count_dev, st);
+    const cudaError_t e2 = cudaFreeAsync(scratch, st);
+    CUDA_TRY(e, "compact");
+    CUDA_TRY(e2, "compact scratch free");
+    return MPM_OK;
+}
+
+mpm_status mpm_raycast(const mpm_ray_params* ray, uint32_t n, const float* pos_in, uint32_t* hit_dev, void* stream) {
+    if (!ray || !hit_dev || (n && !pos_in)) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    CUDA_TRY(launch_raycast(*ray, n, (const float4*)pos_in, hit_dev, (cudaStream_t)stream), "raycast");
     return MPM_OK;
 }
 

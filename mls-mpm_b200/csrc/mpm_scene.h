@@ -75,6 +75,15 @@ struct Scene {
     uint64_t substeps_done = 0;
     uint64_t launches = 0;
 
+    // deleteNear / raycastFluid scratch, allocated on first use (the
+    // reference's particle*Scratch and counter buffers, fluid-gpu.js:230-240)
+    float4* edit_pos = nullptr;
+    float4* edit_vel = nullptr;
+    float* edit_mass = nullptr;
+    uint32_t* edit_blocks = nullptr;   // compact_scratch_words(capacity)
+    uint32_t* edit_word = nullptr;     // device: survivor count / hit bits
+    uint32_t* edit_host = nullptr;     // pinned readback of edit_word
+
     // per-phase CUDA-event profiler (mpm_profile_enable)
     struct Pending { int phase; cudaEvent_t a, b; };
     bool profile = false;

@@ -179,6 +179,11 @@ SIGNATURES = {
     "mpm_default_params": (_I, [_V, _V]),
     "mpm_default_diffuse_params": (_I, [_U32, _V, _V]),
     "mpm_desc_from_aspect": (_I, [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _U32, _V]),
+    "mpm_delete_near": (_I, [_V, _V, _V, ctypes.c_double, ctypes.POINTER(_U32)]),
+    "mpm_raycast_fluid": (_I, [_V, _V, _V, ctypes.c_double, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float), _V]),
+    "mpm_append_particles": (_I, [_V, _V, _V, _V, _U32, ctypes.POINTER(_U32)]),
+    "mpm_compact": (_I, [_V, _U32, _V, _V, _V, _V, _V, _V, _V, _V]),
+    "mpm_raycast": (_I, [_V, _U32, _V, _V, _V]),
 }
 
 PHASE_COUNT = 10

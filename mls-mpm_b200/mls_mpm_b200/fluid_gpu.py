@@ -59,6 +59,7 @@ class FluidGPU:
         self._hand = HandParams()
         self._hand_dims = [0, 0, 0]
         self._params_prev = None
+        self.lastRayHit = None
         self._scene = None
         self._lib = None
 
@@ -157,6 +158,68 @@ class FluidGPU:
         dims = (ctypes.c_int32 * 3)(*self._hand_dims)
         check(self._lib.mpm_set_hand(self._scene, ctypes.byref(self._hand), int(self.handActive), dims),
               "mpm_set_hand")
+
+    # ---- particle editing (fluid-gpu.js:130-179, 529-628) ----
+    def spawnParticles(self, cx, cy, cz, count, radius, vel=(0.0, 0.0, 0.0), sprayVel=3.0, rng=None):
+        """fluid-gpu.js:145-179: up to `count` particles in a jittered sphere with
+        an outward kick, clamped to the hard bounds; returns the number added.
+        rng: a random.Random (the reference uses Math.random)."""
+        rnd = (rng or random).random
+        start = self.active_particle_num
+        n = min(int(count), self.particle_num - start)
+        if n <= 0:
+            return 0
+        pos4 = np.zeros((n, 4), np.float32)
+        vel4 = np.zeros((n, 4), np.float32)
+        hmin, hx, hy, hz = self.HARD_MIN, self.HARD_MAX_X, self.HARD_MAX_Y, self.HARD_MAX_Z
+        for i in range(n):
+            r = radius * math.pow(rnd(), 1.0 / 3.0)
+            theta = rnd() * math.pi * 2
+            cphi = rnd() * 2 - 1
+            sphi = math.sqrt(1 - cphi * cphi)
+            dx, dy, dz = r * sphi * math.cos(theta), r * sphi * math.sin(theta), r * cphi
+            pos4[i, 0] = min(hx, max(hmin, cx + dx))
+            pos4[i, 1] = min(hy, max(hmin, cy + dy))
+            pos4[i, 2] = min(hz, max(hmin, cz + dz))
+            rl = math.hypot(dx, dy, dz) or 1
+            vel4[i, 0] = vel[0] + dx / rl * sprayVel
+            vel4[i, 1] = vel[1] + dy / rl * sprayVel
+            vel4[i, 2] = vel[2] + dz / rl * sprayVel
+        mass = np.ones(n, np.float32)
+        got = ctypes.c_uint32()
+        check(self._lib.mpm_append_particles(self._scene, abi.ptr(pos4), abi.ptr(vel4), abi.ptr(mass), n,
+                                             ctypes.byref(got)), "mpm_append_particles")
+        self.active_particle_num = start + got.value
+        return got.value
+
+    def deleteNear(self, cmd, origin, dir, radius):
+        """fluid-gpu.js:544-571 (+ pollDelete): the new active count is known
+        when the call returns."""
+        self._write_params_buffer(self.DT / self.SUBSTEPS)
+        o = (ctypes.c_double * 3)(*origin)
+        d = (ctypes.c_double * 3)(*dir)
+        m = ctypes.c_uint32()
+        check(self._lib.mpm_delete_near(self._scene, o, d, float(radius), ctypes.byref(m)), "mpm_delete_near")
+        self.active_particle_num = m.value
+        return True
+
+    def pollDelete(self):
+        """fluid-gpu.js:574-584: nothing is pending after deleteNear returns."""
+
+    def raycastFluid(self, cmd, origin, dir, radius):
+        """fluid-gpu.js:594-612 (+ pollRaycast): sets lastRayHit to the world
+        position of the first particle along the ray, or None."""
+        self._write_params_buffer(self.DT / self.SUBSTEPS)
+        o = (ctypes.c_double * 3)(*origin)
+        d = (ctypes.c_double * 3)(*dir)
+        hit, t, hp = ctypes.c_int(), ctypes.c_float(), (ctypes.c_double * 3)()
+        check(self._lib.mpm_raycast_fluid(self._scene, o, d, float(radius), ctypes.byref(hit), ctypes.byref(t), hp),
+              "mpm_raycast_fluid")
+        self.lastRayHit = [hp[0], hp[1], hp[2]] if hit.value else None
+        return True
+
+    def pollRaycast(self):
+        """fluid-gpu.js:615-628: nothing is pending after raycastFluid returns."""
 
     def simFrame(self, cmd=None):
         """fluid-gpu.js:648-684: SUBSTEPS substeps (+ diffuse) on the scene stream."""
