@@ -134,18 +134,22 @@ def test_delete_raycast_append_match_oracle(gpu, engine):
         p.step(6)
         assert p.compare() == []
         # rays: one through the fluid, one that misses, one pointing away
-        for o, d, r in (([12.0, 30.0, 11.0], _unit([0.05, -1.0, 0.02]), 2.0),
+        # (the block fills x 2..12, y 2..14, z 2..5.5)
+        for o, d, r in (([7.0, 30.0, 4.0], _unit([0.05, -1.0, 0.02]), 2.0),
                         ([12.0, 19.5, 11.0], [1.0, 0.0, 0.0], 0.25),
-                        ([12.0, 5.0, -4.0], [0.0, 0.0, -1.0], 3.0)):
+                        ([7.0, 5.0, -4.0], [0.0, 0.0, -1.0], 3.0),
+                        ([-3.0, 6.0, 4.0], [1.0, 0.0, 0.0], 0.5)):
             g, c, hp = p.raycast(o, d, r)
             assert g == c, (o, d, r, hex(g), hex(c))
-        g, c, hp = p.raycast([12.0, 30.0, 11.0], _unit([0.05, -1.0, 0.02]), 2.0)
+        g, c, hp = p.raycast([7.0, 30.0, 4.0], _unit([0.05, -1.0, 0.02]), 2.0)
         assert hp is not None
         t = float(np.uint32(c).view(np.float32))
         d = _unit([0.05, -1.0, 0.02])
-        assert hp == [[12.0, 30.0, 11.0][i] + t * d[i] for i in range(3)]
+        assert hp == [[7.0, 30.0, 4.0][i] + t * d[i] for i in range(3)]
+        g, c, hp = p.raycast([7.0, 5.0, -4.0], [0.0, 0.0, -1.0], 3.0)
+        assert hp is None and c == 0xFFFFFFFF
         # delete a vertical cylinder through the block, then keep stepping
-        m_gpu, m_cpu = p.delete_near([8.0, 10.0, 8.0], _unit([0.1, 1.0, -0.05]), 2.5)
+        m_gpu, m_cpu = p.delete_near([6.0, 10.0, 4.0], _unit([0.1, 1.0, -0.05]), 2.5)
         assert m_gpu == m_cpu and 0 < m_cpu < 3000
         p.step(3)
         assert p.compare() == []
