@@ -207,6 +207,21 @@ mpm_status mpm_compact(const mpm_ray_params* del, uint32_t n, const float* pos_i
 mpm_status mpm_raycast(const mpm_ray_params* ray, uint32_t n, const float* pos_in, uint32_t* hit_dev,
                        void* stream);
 
+/* Largest n mpm_compact_noalloc accepts (its scratch is a fixed 32 KB array). */
+#define MPM_COMPACT_NOALLOC_MAX_N (1u << 24)
+
+/* No counterpart in the reference (whose COMPACT needs no scratch beyond its
+ * atomic counter).  mpm_compact with the same arguments and results, but the
+ * call allocates nothing: the per-block scratch is a fixed device array of
+ * this library.  Runs on the current device.  n > MPM_COMPACT_NOALLOC_MAX_N
+ * fails with MPM_ERR_CAPACITY before any work is enqueued.  The first call on
+ * a device does a one-time setup (looks up the array's address), so make it
+ * outside any stream capture.  Calls on one device share the scratch: calls
+ * that can overlap in time (different streams, unordered threads) race. */
+mpm_status mpm_compact_noalloc(const mpm_ray_params* del, uint32_t n, const float* pos_in, const float* vel_in,
+                               const float* mass_in, float* pos_out, float* vel_out, float* mass_out,
+                               uint32_t* count_dev, void* stream);
+
 /* ---- tracing (no counterpart in the reference, whose only timers are
  * render-pass timestamps, fluid-renderer.js:34-41) ---- */
 

@@ -184,7 +184,10 @@ SIGNATURES = {
     "mpm_append_particles": (_I, [_V, _V, _V, _V, _U32, ctypes.POINTER(_U32)]),
     "mpm_compact": (_I, [_V, _U32, _V, _V, _V, _V, _V, _V, _V, _V]),
     "mpm_raycast": (_I, [_V, _U32, _V, _V, _V]),
+    "mpm_compact_noalloc": (_I, [_V, _U32, _V, _V, _V, _V, _V, _V, _V, _V]),
 }
+
+COMPACT_NOALLOC_MAX_N = 1 << 24
 
 PHASE_COUNT = 10
 
