@@ -103,11 +103,15 @@ static void free_scene(Scene& s) {
     for (cudaEvent_t e : s.event_pool) cudaEventDestroy(e);
     s.pending.clear();
     s.event_pool.clear();
-    fast_free(s.fast);
+    if (s.engine == kEngineBinned) {
+        world_free(s.world);   // owns cmf/mvf of the binned engine
+        s.cmf = nullptr;
+        s.mvf = nullptr;
+    }
     void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
                     s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
                     s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.rank_state, s.diffuse.staging,
-                    s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word};
+                    s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word, s.diffuse.gen_dev};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s.diffuse.host_top) cudaFreeHost(s.diffuse.host_top);
@@ -135,9 +139,14 @@ static bool buffer_info(Scene& s, mpm_buffer which, void** ptr, size_t* bytes) {
         case MPM_BUF_MASS: *ptr = s.mass; *bytes = N * 4; return true;
         case MPM_BUF_DENSITY: *ptr = s.dens; *bytes = N * 4; return true;
         case MPM_BUF_CELL_MV:
-            *ptr = s.engine == kEnginePlain ? s.mv : s.fast.cm_current + G; *bytes = G * 12; return true;
-        case MPM_BUF_CELL_MASS:
-            *ptr = s.engine == kEnginePlain ? s.cm : s.fast.cm_current; *bytes = G * 4; return true;
+        case MPM_BUF_CELL_MASS: {
+            int32_t* cm = s.cm;
+            int32_t* mv = s.mv;
+            if (s.engine == kEngineBinned) world_scene_grid(s.world, s.world_slot, &cm, &mv, nullptr, nullptr);
+            *ptr = which == MPM_BUF_CELL_MV ? (void*)mv : (void*)cm;
+            *bytes = which == MPM_BUF_CELL_MV ? G * 12 : G * 4;
+            return true;
+        }
         case MPM_BUF_CELL_MV_F32: *ptr = s.mvf; *bytes = G * 12; return true;
         case MPM_BUF_CELL_MASS_F32: *ptr = s.cmf; *bytes = G * 4; return true;
         case MPM_BUF_DIFFUSE:
@@ -160,16 +169,21 @@ static bool is_particle_buffer(mpm_buffer w) {
 // Binned engine: bring the reference-layout particle buffers up to date.
 static cudaError_t sync_reference_buffers(Scene& s) {
     if (s.engine != kEngineBinned || !s.ref_stale) return cudaSuccess;
-    cudaError_t e = fast_export(s.fast, s.pos, s.vel, s.aff, s.mass, s.fast.dens_valid ? s.dens : nullptr, s.stream);
+    cudaError_t e = world_export_scene(s.world, s.world_slot, s.pos, s.vel, s.aff, s.mass, s.dens);
     if (e == cudaSuccess) s.ref_stale = false;
     return e;
 }
 
 // Binned engine: (re)load the working state from the reference-layout buffers.
 static cudaError_t import_state(Scene& s) {
-    cudaError_t e = fast_import(s.fast, s.pos, s.vel, s.aff, s.mass, s.params.particle_num, s.stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s.cmf, 0, s.G * 4, s.stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s.mvf, 0, s.G * 12, s.stream);
+    // drop the scene from its world and add it back with the buffers' particles
+    // (this also zeroes its grids, as a fresh load does)
+    cudaError_t e = cudaSuccess;
+    if (s.world_slot >= 0) e = world_remove_scene(s.world, s.world_slot);
+    s.world_slot = -1;
+    if (e == cudaSuccess)
+        e = world_add_scene(s.world, s.X, s.Y, s.Z, s.params, s.walls, s.pos, s.vel, s.aff, s.mass,
+                            s.params.particle_num, &s.world_slot);
     if (e == cudaSuccess) s.fast_stale = false;
     return e;
 }
@@ -178,7 +192,8 @@ static cudaError_t launch_substep(Scene& s) {
     s.substeps_done++;
     if (s.engine == kEnginePlain) return launch_substep_plain(s);
     s.ref_stale = true;
-    return fast_substep(s);
+    world_set_uniforms(s.world, s.world_slot, s.params, s.walls, &s.hand, s.hand_active, s.hand_dims);
+    return world_substep(s.world, &s, true);
 }
 
 }  // namespace mpm
@@ -283,9 +298,13 @@ mpm_status mpm_create(const mpm_desc* d, mpm_scene** out) {
     if (e == cudaSuccess) e = dalloc(&s.mass, N * 4);
     if (e == cudaSuccess) e = dalloc(&s.dens, N * 4);
     if (e == cudaSuccess && s.engine == kEnginePlain) e = dalloc(&s.grid_i32, G * 16);
-    if (e == cudaSuccess && s.engine == kEngineBinned) e = fast_alloc(s.fast, s.X, s.Y, s.Z, s.capacity, s.device);
-    if (e == cudaSuccess) e = dalloc(&s.cmf, G * 4);
-    if (e == cudaSuccess) e = dalloc(&s.mvf, G * 12);
+    if (e == cudaSuccess && s.engine == kEngineBinned) e = world_alloc(s.world, s.device, s.stream, s.capacity, G, 1);
+    if (e == cudaSuccess && s.engine == kEnginePlain) e = dalloc(&s.cmf, G * 4);
+    if (e == cudaSuccess && s.engine == kEnginePlain) e = dalloc(&s.mvf, G * 12);
+    if (e == cudaSuccess && s.engine == kEngineBinned) {
+        s.cmf = s.world.cmf;
+        s.mvf = s.world.mvf;
+    }
     if (e != cudaSuccess) {
         free_scene(s);
         delete sc;
@@ -302,7 +321,14 @@ mpm_status mpm_create(const mpm_desc* d, mpm_scene** out) {
     cudaMemsetAsync(s.mass, 0, N * 4, s.stream);
     cudaMemsetAsync(s.dens, 0, N * 4, s.stream);
     if (s.grid_i32) cudaMemsetAsync(s.grid_i32, 0, G * 16, s.stream);
-    if (s.engine == kEngineBinned) fast_import(s.fast, s.pos, s.vel, s.aff, s.mass, 0, s.stream);
+    if (s.engine == kEngineBinned) {
+        e = import_state(s);
+        if (e != cudaSuccess) {
+            free_scene(s);
+            delete sc;
+            return cuda_fail(e, "mpm_create world");
+        }
+    }
     cudaMemsetAsync(s.cmf, 0, G * 4, s.stream);
     cudaMemsetAsync(s.mvf, 0, G * 12, s.stream);
     e = cudaStreamSynchronize(s.stream);
@@ -353,7 +379,7 @@ mpm_status mpm_set_params(mpm_scene* sc, const mpm_params* p) {
     if (p->grid_X != s.X || p->grid_Y != s.Y || p->grid_Z != s.Z)
         return fail(MPM_ERR_INVALID_ARG, "params grid dims differ from the scene's");
     if (p->particle_num > s.capacity) return fail(MPM_ERR_CAPACITY, "particle_num exceeds capacity");
-    if (s.engine == kEngineBinned && p->particle_num != s.fast.n) {
+    if (s.engine == kEngineBinned && s.world_slot >= 0 && p->particle_num != s.world.scenes[s.world_slot].n) {
         // active count changed (spawn / delete): reload the working state next step
         DeviceGuard guard(s.device);
         CUDA_TRY(sync_reference_buffers(s), "export");
@@ -398,6 +424,7 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     if (e == cudaSuccess) e = dalloc(&d.block_counts, nb * 4);
     if (e == cudaSuccess) e = dalloc(&d.rank_state, 16);
     if (e == cudaSuccess) e = dalloc(&d.staging, N * 48);
+    if (e == cudaSuccess) e = dalloc(&d.gen_dev, sizeof(mpm_gen_params));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&d.host_top, 16);
     if (e != cudaSuccess) return cuda_fail(e, "mpm_diffuse_enable allocation");
     // diffuse-gpu.js:60-68: free list [0..M-1], top = M, all slots dead
@@ -413,6 +440,8 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     d.adv = *adv;
     d.adv.diffuse_max = (uint32_t)M;
     d.seed = gen->seed;
+    CUDA_TRY(cudaMemcpyAsync(d.gen_dev, &d.gen, sizeof(mpm_gen_params), cudaMemcpyHostToDevice, s.stream),
+             "gen params");
     d.enabled = true;
     return MPM_OK;
 }
@@ -420,8 +449,12 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
 mpm_status mpm_diffuse_set_gen_params(mpm_scene* sc, const mpm_gen_params* gen) {
     if (!sc || !gen) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     if (!sc->s.diffuse.enabled) return fail(MPM_ERR_INVALID_ARG, "diffuse not enabled");
-    sc->s.diffuse.gen = *gen;
-    sc->s.diffuse.seed = gen->seed;
+    DiffuseState& d = sc->s.diffuse;
+    d.gen = *gen;
+    d.seed = gen->seed;
+    DeviceGuard guard(sc->s.device);
+    CUDA_TRY(cudaMemcpyAsync(d.gen_dev, gen, sizeof(mpm_gen_params), cudaMemcpyHostToDevice, sc->s.stream),
+             "gen params");
     return MPM_OK;
 }
 
@@ -658,7 +691,7 @@ mpm_status mpm_profile_read(mpm_scene* sc, double* ms, uint64_t* count, int rese
 
 mpm_status mpm_launch_count(mpm_scene* sc, uint64_t* launches) {
     if (!sc || !launches) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
-    *launches = sc->s.launches + sc->s.fast.launches;
+    *launches = sc->s.launches + sc->s.world.launches;
     return MPM_OK;
 }
 

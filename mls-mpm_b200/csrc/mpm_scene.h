@@ -8,7 +8,7 @@
 #include <vector>
 
 #include "../../include/mpm_b200.h"
-#include "mpm_fast.h"
+#include "mpm_world.h"
 
 namespace mpm {
 
@@ -33,6 +33,7 @@ struct DiffuseState {
     int32_t* rank_state = nullptr;          // [0] = top before the pass, [1] = total, [2] = applied
     mpm_diffuse_particle* staging = nullptr;  // N x 48 B spawn records indexed by particle id
     int32_t* host_top = nullptr;            // pinned 4 B for alive-count readback
+    mpm_gen_params* gen_dev = nullptr;      // device GenParams (binned engine: seed bumped on the device)
 };
 
 // Engines: the binned item-major substep (default) and the plain per-pass
@@ -68,7 +69,8 @@ struct Scene {
     float* mvf = nullptr;
 
     DiffuseState diffuse;
-    FastEngine fast;
+    World world;              // binned engine: a world holding this one scene
+    int world_slot = -1;
     // binned engine: which copy of the particle state is newer
     bool ref_stale = false;    // reference-layout buffers behind the binned state
     bool fast_stale = false;   // binned state behind the reference-layout buffers
@@ -102,11 +104,16 @@ void set_error(const std::string& msg);
 
 // RAII phase marker: records a start/end event pair when profiling is on.
 struct Phase {
-    Scene& s;
+    Scene* s;
     int ph;
     cudaEvent_t a = nullptr;
-    Phase(Scene& sc, int p) : s(sc), ph(p) { s.begin_phase(ph, &a); }
-    ~Phase() { s.end_phase(ph, a); }
+    Phase(Scene& sc, int p) : s(&sc), ph(p) { s->begin_phase(ph, &a); }
+    Phase(Scene* sc, int p) : s(sc), ph(p) {   // null: not profiled
+        if (s) s->begin_phase(ph, &a);
+    }
+    ~Phase() {
+        if (s) s->end_phase(ph, a);
+    }
 };
 
 }  // namespace mpm

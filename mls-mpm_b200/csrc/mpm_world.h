@@ -1,0 +1,194 @@
+// mpm_world.h — the binned, item-major engine over a world of scenes.
+//
+// A world holds any number of independent scenes (each its own grid, params
+// and walls) in shared device arrays: every scene owns a range of global
+// cells, a range of global tiles and a range of particle ids; particles of
+// all scenes share one position space, one set of length buckets and one
+// launch per kernel per substep.  A single scene is a world of one.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/mpm_types.h"
+
+namespace mpm {
+
+// Grid tile (cells) used by the sparse grid passes and the binning.
+constexpr int kTileX = 16, kTileY = 8, kTileZ = 8;
+constexpr int kTileCells = kTileX * kTileY * kTileZ;   // 1024: one thread per cell in k_bin_cells
+
+// A cell's particles are split into work items of at most kMaxL particles;
+// items are grouped by length into buckets 1..kMaxL so that the 32 lanes of a
+// warp always run the same number of iterations.
+constexpr int kMaxL = 16;
+// Positions lost to padding the last warp of each bucket: 31 * (1 + ... + kMaxL).
+constexpr uint32_t kPosSlack = 31u * (kMaxL * (kMaxL + 1) / 2) + 64u;
+constexpr uint32_t kHole = 0xFFFFFFFFu;   // key / id of a padding position
+
+// Device scene table entry (read by the kernels).
+struct alignas(16) SceneDesc {
+    uint32_t X, Y, Z, G;
+    uint32_t cell_base, tile_base, ntx, nty;
+    uint32_t ntz, id_base, n, flags;
+    int32_t hand_box[6];        // cells APPLY_HAND may write this substep (x0 > x1: none)
+    uint32_t pad[2];
+    mpm_params P;
+    mpm_wall_params W;
+    mpm_hand_params H;          // APPLY_HAND uniform, applied inside UPDATE_GRID over hand_box
+};
+
+// Small device-side control block.  The first kCtrlZeroBytes are cleared at
+// the start of every substep.
+struct Ctrl {
+    uint32_t n_occ, n_grid, pad0, pad1;
+    uint32_t tail_cnt[kMaxL + 1];            // items of overpacked cells per length (unordered)
+    uint32_t pad2[64 - 4 - (kMaxL + 1)];
+    // persistent
+    uint32_t bucket_reg[kMaxL + 2];          // ordered items per length (one per cell with 1..kMaxL particles)
+    uint32_t bucket_cnt[kMaxL + 2];          // ordered + tail items per length
+    uint32_t item_off[kMaxL + 2];            // first padded item index of each bucket
+    uint32_t pos_off[kMaxL + 2];             // first position of each bucket
+    uint32_t total_items, total_pos, prev_total_pos, pad3;
+};
+constexpr size_t kCtrlZeroBytes = 64 * 4;
+
+// Everything the device kernels need (passed by value).
+struct WorldView {
+    uint32_t npos;             // capacity of the position space
+    uint32_t ntiles;           // tiles in use (end of the allocated tile range)
+    uint32_t nchunks;          // ceil(ntiles / 1024): chunks of the two-level tile scan
+    uint32_t cap_off[kMaxL + 2];   // start of each bucket's item list in bucket_items
+    const SceneDesc* scenes;
+    const uint32_t* tile_scene;    // scene of each global tile (kHole: free)
+    uint32_t* cell_count;      // total cells + 1, zero outside binning
+    uint4* cell_info;          // per cell: (L | Llast<<8 | q<<16 | overpacked<<31, idx, idxLast|tile, scene)
+    uint2* bucket_items;       // (cell, scene) of each item, per bucket
+    uint32_t* key;             // npos: binning cell (global) of each position of the current state, or kHole
+    uint32_t* rank;            // npos: rank within the cell
+    uint32_t* perm;            // npos: position -> position of the previous layout
+    uint32_t* tile_flags;      // per tile
+    uint32_t* tile_occ;        // per tile: 1 if the tile holds particles this substep
+    uint32_t* tile_hist;       // kMaxL x tiles: ordered items per (length, tile)
+    uint32_t* tile_base_;      // kMaxL x tiles: exclusive scan of tile_hist inside each 1024-tile chunk
+    uint32_t* tile_chunk;      // kMaxL x nchunks: exclusive scan of the chunk totals
+    uint32_t* tile_occ_list;
+    uint32_t* tile_grid_list;
+    Ctrl* ctrl;
+    float* dens;               // npos, layout of the last substep
+};
+
+// Diffuse spawn staging for the one scene of a world that has diffuse on.
+struct DiffuseView {
+    int enabled;
+    uint32_t scene;
+    const mpm_gen_params* gen;       // device copy; seed bumped on the device each substep
+    mpm_diffuse_particle* staging;   // by particle id
+    uint32_t* spawn_bits;            // by particle id
+};
+
+// Host record of a scene in a world.
+struct SceneRec {
+    bool live = false;
+    uint32_t X = 0, Y = 0, Z = 0;
+    uint32_t cell_base = 0, G = 0, tile_base = 0, ntiles = 0, id_base = 0, n = 0, id_cap = 0;
+    mpm_params P{};
+    mpm_wall_params W{};
+    int32_t hand_box[6] = {1, 1, 1, 0, 0, 0};
+    mpm_hand_params H{};
+};
+
+// First-fit range allocator (host side) for cells, tiles and ids.
+struct RangeAlloc {
+    uint64_t cap = 0;
+    std::vector<std::pair<uint64_t, uint64_t>> free_;   // (start, len), sorted
+    void reset(uint64_t c) { cap = c; free_.assign(1, {0, c}); }
+    bool alloc(uint64_t len, uint64_t& start);
+    void release(uint64_t start, uint64_t len);
+    uint64_t high_water() const;   // end of the last allocated range
+};
+
+struct World {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t pcap = 0, npos = 0;            // particle capacity, position capacity
+    uint64_t cell_cap = 0;
+    uint32_t tile_cap = 0, id_cap = 0, scene_cap = 0;
+    uint32_t item_blocks = 0, grid_blocks = 0, bin_blocks = 0, pos_blocks = 0;
+    uint32_t cap_off[kMaxL + 2] = {};
+    std::vector<SceneRec> scenes;           // by scene slot
+    RangeAlloc cells, tiles, ids;
+    uint32_t n_total = 0;                   // particles in all scenes
+    uint32_t pos_bound = 0;                 // host bound on the layout end (device ctrl->total_pos)
+    int cur = 0;                            // particle state copy holding the latest state
+    int gbuf = 0;                           // i32 grid buffer the next substep accumulates into
+    bool dens_valid = false;
+    bool table_dirty = true;
+    uint64_t launches = 0;
+    uint64_t generation = 1;                // bumps whenever the captured launch arguments change
+
+    // device arrays
+    SceneDesc* d_scenes = nullptr;
+    std::vector<SceneDesc> h_scenes;        // host copy of the table (pageable, see world_upload_table)
+    uint32_t* tile_scene = nullptr;
+    std::vector<uint32_t> h_tile_scene;
+    float4* posm[2] = {nullptr, nullptr};   // (x, y, z, mass)
+    float4* velid[2] = {nullptr, nullptr};  // (vx, vy, vz, id bits)
+    float* aff[2] = {nullptr, nullptr};     // 9 planes of npos floats
+    float* dens = nullptr;
+    uint32_t* cell_count = nullptr;
+    uint4* cell_info = nullptr;
+    uint2* bucket_items = nullptr;
+    uint32_t* key = nullptr;
+    uint32_t* rank = nullptr;
+    uint32_t* perm = nullptr;
+    uint32_t* tile_flags = nullptr;
+    uint32_t* tile_occ = nullptr;
+    uint32_t* tile_hist = nullptr;
+    uint32_t* tile_base = nullptr;
+    uint32_t* tile_chunk = nullptr;
+    uint32_t* tile_occ_list = nullptr;
+    uint32_t* tile_grid_list = nullptr;
+    Ctrl* ctrl = nullptr;
+    int32_t* grid_i32[2] = {nullptr, nullptr};   // each [cm: cells][mv: 3 cells]
+    int32_t* cm_current = nullptr;               // buffer holding the last substep's P2G sums
+    float* cmf = nullptr;                        // cells
+    float* mvf = nullptr;                        // 3 cells
+
+    // CUDA graphs of one substep (one per buffer parity), valid for `generation`
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint64_t graph_gen[2] = {0, 0};
+    uint64_t graph_kernels[2] = {0, 0};     // kernels in each graph (launch accounting)
+
+    WorldView view() const;
+};
+
+cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t particle_cap, uint64_t cell_cap,
+                        uint32_t scene_cap);
+void world_free(World& w);
+// Adds a scene (grid dims, params, walls) with particles from reference-layout
+// device buffers (pos4, vel4 or null, affine9 or null, mass); returns its slot.
+cudaError_t world_add_scene(World& w, uint32_t X, uint32_t Y, uint32_t Z, const mpm_params& P,
+                            const mpm_wall_params& W, const float4* pos, const float4* vel, const float* aff,
+                            const float* mass, uint32_t n, int* slot);
+cudaError_t world_remove_scene(World& w, int slot);
+// Writes a scene's particles (reference layouts, by local id) to device buffers.
+cudaError_t world_export_scene(World& w, int slot, float4* pos, float4* vel, float* aff, float* mass, float* dens);
+// Grid buffers of a scene (reference layouts) inside the world arrays.
+void world_scene_grid(const World& w, int slot, int32_t** cm, int32_t** mv, float** cmf, float** mvf);
+cudaError_t world_upload_table(World& w);
+// Sets a scene's uniforms (Params, WallParams, HandParams + dispatch dims;
+// hand_dims null or active == 0: no APPLY_HAND).  Takes effect at the next substep.
+void world_set_uniforms(World& w, int slot, const mpm_params& P, const mpm_wall_params& W,
+                        const mpm_hand_params* H, int hand_active, const int32_t* hand_dims);
+
+struct Scene;
+// One substep of every scene.  diffuse_owner: the single-scene wrapper whose
+// diffuse pool follows scene slot 0 (null: no diffuse).  use_graph: replay a
+// captured CUDA graph of the substep (captured on first use and whenever the
+// scene set changes).
+cudaError_t world_substep(World& w, Scene* diffuse_owner, bool use_graph);
+
+}  // namespace mpm
