@@ -254,6 +254,77 @@ mpm_status mpm_profile_read(mpm_scene* scene, double* ms, uint64_t* count, int r
 /* Number of kernels this scene has launched (CUDA kernels only). */
 mpm_status mpm_launch_count(mpm_scene* scene, uint64_t* launches);
 
+/* ---- batching: many independent scenes advanced together (no counterpart
+ * in the reference, which runs one FluidGPU per page).  Every kernel of a
+ * substep runs once for all scenes of the batch over a device table of
+ * per-scene grid dims, Params, WallParams and HandParams; results per scene
+ * are bit-identical to the same scene run alone.  No diffuse in batches. ---- */
+
+typedef struct mpm_batch mpm_batch;
+
+/* mpm_batch_desc.flags: step without CUDA graphs (one launch per kernel). */
+#define MPM_BATCH_NO_GRAPH 1u
+/* mpm_batch_desc.flags: time the first substeps of each workload under
+ * several launch shapes and keep the fastest (results do not depend on it). */
+#define MPM_BATCH_AUTOTUNE 2u
+
+typedef struct mpm_batch_desc {
+    uint32_t particle_capacity;   /* particles over all scenes at once */
+    uint32_t scene_capacity;      /* scenes at once */
+    uint64_t cell_capacity;       /* grid cells over all scenes at once */
+    int32_t device;               /* CUDA device ordinal */
+    uint32_t flags;               /* MPM_BATCH_* */
+} mpm_batch_desc;
+
+typedef struct mpm_batch_info {
+    uint32_t scenes;              /* live scenes */
+    uint32_t particles;           /* particles over live scenes */
+    uint64_t cells;               /* cells over live scenes */
+    uint64_t launches;            /* kernels launched so far */
+    uint64_t substeps;            /* batch substeps run so far */
+    uint64_t device_bytes;        /* device memory held by the batch */
+    uint32_t item_blocks, grid_blocks;   /* launch shape in use */
+} mpm_batch_info;
+
+/* Device bytes mpm_batch_create would allocate for these capacities (for
+ * admission against an HBM budget). */
+mpm_status mpm_batch_footprint(uint32_t particle_capacity, uint64_t cell_capacity, uint32_t scene_capacity,
+                               uint64_t* bytes);
+
+mpm_status mpm_batch_create(const mpm_batch_desc* desc, mpm_batch** out);
+mpm_status mpm_batch_destroy(mpm_batch* batch);
+
+/* Adds a scene: `params` as mpm_set_params gives them (grid_X/Y/Z set the
+ * scene's grid, at least 5 per axis; particle_num is replaced by n), walls
+ * may be NULL (none), host particle arrays as mpm_upload_particles takes
+ * them.  *scene receives the scene id.  MPM_ERR_CAPACITY when particles,
+ * cells or scene slots are exhausted; MPM_ERR_BUSY when the particle layout
+ * still holds removed scenes' slots (step once, then add). */
+mpm_status mpm_batch_add(mpm_batch* batch, const mpm_params* params, const mpm_wall_params* walls,
+                         const float* pos4, const float* vel4, const float* affine9, const float* mass, uint32_t n,
+                         int32_t* scene);
+
+/* Removes a scene and frees its particles, cells and id range. */
+mpm_status mpm_batch_remove(mpm_batch* batch, int32_t scene);
+
+/* Per-scene uniforms, as mpm_set_params / mpm_set_walls / mpm_set_hand
+ * (grid dims must equal the scene's; particle_num is ignored). */
+mpm_status mpm_batch_set_params(mpm_batch* batch, int32_t scene, const mpm_params* params);
+mpm_status mpm_batch_set_walls(mpm_batch* batch, int32_t scene, const mpm_wall_params* walls);
+mpm_status mpm_batch_set_hand(mpm_batch* batch, int32_t scene, const mpm_hand_params* hand, int active,
+                              const int32_t bbox_dims[3]);
+
+/* Advances every scene by `substeps` substeps; enqueues and returns. */
+mpm_status mpm_batch_step(mpm_batch* batch, int substeps);
+mpm_status mpm_batch_sync(mpm_batch* batch);
+
+/* Copies one buffer of one scene (reference layout, the scene's own particle
+ * ids and grid) to host memory; waits. */
+mpm_status mpm_batch_download(mpm_batch* batch, int32_t scene, mpm_buffer which, void* host_dst, size_t bytes);
+
+mpm_status mpm_batch_get_stream(mpm_batch* batch, void** stream);
+mpm_status mpm_batch_get_info(mpm_batch* batch, mpm_batch_info* info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1211,10 +1211,8 @@ inline uint32_t cdiv(uint64_t a, uint32_t b) { return (uint32_t)((a + b - 1) / b
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t particle_cap, uint64_t cell_cap,
-                        uint32_t scene_cap) {
-    w.device = device;
-    w.stream = stream;
+// Capacities derived from the requested particle / cell / scene counts.
+static void world_plan(World& w, uint32_t particle_cap, uint64_t cell_cap, uint32_t scene_cap) {
     w.pcap = particle_cap;
     w.npos = particle_cap + kPosSlack;
     w.cell_cap = cell_cap;
@@ -1223,10 +1221,6 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
     w.tile_cap = (uint32_t)(3 * (cell_cap / kTileCells)) + 64u * scene_cap + 64u;
     w.id_cap = particle_cap;
     w.scene_cap = scene_cap;
-    w.cells.reset(cell_cap);
-    w.tiles.reset(w.tile_cap);
-    w.ids.reset(particle_cap ? particle_cap : 1);
-    w.scenes.assign(scene_cap, SceneRec());
     uint32_t off = 0;
     w.cap_off[0] = 0;
     for (int b = 1; b <= kMaxL; ++b) {
@@ -1234,42 +1228,73 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
         off += w.npos / b + 1;
     }
     w.cap_off[kMaxL + 1] = off;
+}
+
+// Every device array of a world with its size (one list for allocation,
+// release and the footprint).
+template <class F> static void world_arrays(World& w, F&& f) {
+    const size_t P = w.npos, C = w.cell_cap ? w.cell_cap : 1, T = w.tile_cap;
+    for (int b = 0; b < 2; ++b) {
+        f(w.posm[b], P * 16);
+        f(w.velid[b], P * 16);
+        f(w.aff[b], P * 36);
+        f(w.grid_i32[b], C * 16);
+    }
+    f(w.dens, P * 4);
+    f(w.cell_count, (C + 1) * 4);
+    f(w.cell_info, C * 16);
+    f(w.bucket_items, (size_t)w.cap_off[kMaxL + 1] * 8);
+    f(w.key, P * 4);
+    f(w.rank, P * 4);
+    f(w.perm, P * 4);
+    f(w.tile_flags, T * 4);
+    f(w.tile_occ, T * 4);
+    f(w.tile_hist, (size_t)kMaxL * T * 4);
+    f(w.tile_base, (size_t)kMaxL * T * 4);
+    f(w.tile_chunk, (size_t)kMaxL * ((T + 1023) / 1024 + 1) * 4);
+    f(w.tile_occ_list, T * 4);
+    f(w.tile_grid_list, T * 4);
+    f(w.tile_scene, T * 4);
+    f(w.ctrl, sizeof(Ctrl));
+    f(w.cmf, C * 4);
+    f(w.mvf, C * 12);
+    f(w.d_scenes, (size_t)w.scene_cap * sizeof(SceneDesc));
+}
+
+uint64_t world_footprint(uint32_t particle_cap, uint64_t cell_cap, uint32_t scene_cap) {
+    World w;
+    world_plan(w, particle_cap, cell_cap, scene_cap);
+    uint64_t total = 0;
+    world_arrays(w, [&](auto*& p, size_t bytes) {
+        (void)p;
+        total += (bytes + 511) & ~(uint64_t)511;   // allocation granularity
+    });
+    return total;
+}
+
+cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t particle_cap, uint64_t cell_cap,
+                        uint32_t scene_cap) {
+    w.device = device;
+    w.stream = stream;
+    world_plan(w, particle_cap, cell_cap, scene_cap);
+    w.cells.reset(cell_cap);
+    w.tiles.reset(w.tile_cap);
+    w.ids.reset(particle_cap ? particle_cap : 1);
+    w.scenes.assign(scene_cap, SceneRec());
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    w.sms = (uint32_t)sms;
     w.item_blocks = (uint32_t)sms * 8;
     w.grid_blocks = (uint32_t)sms * 8;
     w.bin_blocks = (uint32_t)sms * 2;
     w.pos_blocks = std::min<uint32_t>(cdiv(w.npos, 256), (uint32_t)sms * 16);
     const size_t P = w.npos, C = cell_cap ? cell_cap : 1, T = w.tile_cap;
     cudaError_t e = cudaSuccess;
-    auto A = [&](auto** p, size_t bytes) {
-        if (e == cudaSuccess) e = cudaMalloc((void**)p, bytes ? bytes : 16);
-    };
-    for (int b = 0; b < 2; ++b) {
-        A(&w.posm[b], P * 16);
-        A(&w.velid[b], P * 16);
-        A(&w.aff[b], P * 36);
-        A(&w.grid_i32[b], C * 16);
-    }
-    A(&w.dens, P * 4);
-    A(&w.cell_count, (C + 1) * 4);
-    A(&w.cell_info, C * 16);
-    A(&w.bucket_items, (size_t)off * 8);
-    A(&w.key, P * 4);
-    A(&w.rank, P * 4);
-    A(&w.perm, P * 4);
-    A(&w.tile_flags, T * 4);
-    A(&w.tile_occ, T * 4);
-    A(&w.tile_hist, (size_t)kMaxL * T * 4);
-    A(&w.tile_base, (size_t)kMaxL * T * 4);
-    A(&w.tile_chunk, (size_t)kMaxL * ((T + 1023) / 1024 + 1) * 4);
-    A(&w.tile_occ_list, T * 4);
-    A(&w.tile_grid_list, T * 4);
-    A(&w.tile_scene, T * 4);
-    A(&w.ctrl, sizeof(Ctrl));
-    A(&w.cmf, C * 4);
-    A(&w.mvf, C * 12);
-    A(&w.d_scenes, (size_t)scene_cap * sizeof(SceneDesc));
+    w.device_bytes = 0;
+    world_arrays(w, [&](auto*& p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc((void**)&p, bytes ? bytes : 16);
+        if (e == cudaSuccess) w.device_bytes += bytes;
+    });
     if (e != cudaSuccess) return e;
     w.h_scenes.assign(scene_cap, SceneDesc{});
     w.h_tile_scene.assign(T, kHole);
@@ -1296,14 +1321,18 @@ void world_free(World& w) {
     if (w.stream) cudaStreamSynchronize(w.stream);
     for (int b = 0; b < 2; ++b)
         if (w.graph[b]) cudaGraphExecDestroy(w.graph[b]);
-    void* ptrs[] = {w.posm[0], w.posm[1], w.velid[0], w.velid[1], w.aff[0], w.aff[1], w.grid_i32[0],
-                    w.grid_i32[1], w.dens, w.cell_count, w.cell_info, w.bucket_items, w.key, w.rank, w.perm,
-                    w.tile_flags, w.tile_occ, w.tile_hist, w.tile_base, w.tile_chunk, w.tile_occ_list,
-                    w.tile_grid_list,
-                    w.tile_scene, w.ctrl, w.cmf, w.mvf, w.d_scenes};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    world_arrays(w, [](auto*& p, size_t) {
+        if (p) cudaFree((void*)p);
+        p = nullptr;
+    });
     w = World();
+}
+
+void world_set_launch_shape(World& w, uint32_t item_blocks, uint32_t grid_blocks) {
+    if (item_blocks == w.item_blocks && grid_blocks == w.grid_blocks) return;
+    w.item_blocks = item_blocks;
+    w.grid_blocks = grid_blocks;
+    w.generation++;   // captured graphs hold the old shape
 }
 
 static void fill_desc(World& w, int slot) {

@@ -116,7 +116,9 @@ struct World {
     uint32_t pcap = 0, npos = 0;            // particle capacity, position capacity
     uint64_t cell_cap = 0;
     uint32_t tile_cap = 0, id_cap = 0, scene_cap = 0;
+    uint32_t sms = 0;
     uint32_t item_blocks = 0, grid_blocks = 0, bin_blocks = 0, pos_blocks = 0;
+    uint64_t device_bytes = 0;              // device memory of the arrays below
     uint32_t cap_off[kMaxL + 2] = {};
     std::vector<SceneRec> scenes;           // by scene slot
     RangeAlloc cells, tiles, ids;
@@ -168,6 +170,10 @@ struct World {
 cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t particle_cap, uint64_t cell_cap,
                         uint32_t scene_cap);
 void world_free(World& w);
+// Device bytes world_alloc takes for these capacities.
+uint64_t world_footprint(uint32_t particle_cap, uint64_t cell_cap, uint32_t scene_cap);
+// Grid sizes of the item kernels and the tile passes (results do not depend on them).
+void world_set_launch_shape(World& w, uint32_t item_blocks, uint32_t grid_blocks);
 // Adds a scene (grid dims, params, walls) with particles from reference-layout
 // device buffers (pos4, vel4 or null, affine9 or null, mass); returns its slot.
 cudaError_t world_add_scene(World& w, uint32_t X, uint32_t Y, uint32_t Z, const mpm_params& P,

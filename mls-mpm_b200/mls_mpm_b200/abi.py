@@ -185,7 +185,34 @@ SIGNATURES = {
     "mpm_compact": (_I, [_V, _U32, _V, _V, _V, _V, _V, _V, _V, _V]),
     "mpm_raycast": (_I, [_V, _U32, _V, _V, _V]),
     "mpm_compact_noalloc": (_I, [_V, _U32, _V, _V, _V, _V, _V, _V, _V, _V]),
+    "mpm_batch_footprint": (_I, [_U32, _U64, _U32, ctypes.POINTER(_U64)]),
+    "mpm_batch_create": (_I, [_V, ctypes.POINTER(_V)]),
+    "mpm_batch_destroy": (_I, [_V]),
+    "mpm_batch_add": (_I, [_V, _V, _V, _V, _V, _V, _V, _U32, ctypes.POINTER(ctypes.c_int32)]),
+    "mpm_batch_remove": (_I, [_V, ctypes.c_int32]),
+    "mpm_batch_set_params": (_I, [_V, ctypes.c_int32, _V]),
+    "mpm_batch_set_walls": (_I, [_V, ctypes.c_int32, _V]),
+    "mpm_batch_set_hand": (_I, [_V, ctypes.c_int32, _V, _I, _V]),
+    "mpm_batch_step": (_I, [_V, _I]),
+    "mpm_batch_sync": (_I, [_V]),
+    "mpm_batch_download": (_I, [_V, ctypes.c_int32, _I, _V, _SZ]),
+    "mpm_batch_get_stream": (_I, [_V, ctypes.POINTER(_V)]),
+    "mpm_batch_get_info": (_I, [_V, _V]),
 }
+
+BATCH_NO_GRAPH = 1
+BATCH_AUTOTUNE = 2
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("particle_capacity", ctypes.c_uint32), ("scene_capacity", ctypes.c_uint32),
+                ("cell_capacity", ctypes.c_uint64), ("device", ctypes.c_int32), ("flags", ctypes.c_uint32)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("scenes", ctypes.c_uint32), ("particles", ctypes.c_uint32), ("cells", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("substeps", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64),
+                ("item_blocks", ctypes.c_uint32), ("grid_blocks", ctypes.c_uint32)]
 
 COMPACT_NOALLOC_MAX_N = 1 << 24
 

@@ -76,3 +76,16 @@ def test_create_without_device_is_an_error_not_a_fallback(native):
     h = ctypes.c_void_p()
     assert native.mpm_create(ctypes.byref(d), ctypes.byref(h)) == 6   # MPM_ERR_NO_DEVICE
     assert not h.value
+
+
+def test_batch_footprint_without_device(native):
+    """mpm_batch_footprint is host arithmetic: usable for admission before any device work."""
+    import ctypes
+    out = []
+    for p, c, s in ((1 << 20, 1 << 21, 1), (1 << 22, 1 << 21, 64), (1 << 22, 1 << 23, 64)):
+        b = ctypes.c_uint64()
+        assert native.mpm_batch_footprint(p, c, s, ctypes.byref(b)) == 0
+        out.append(b.value)
+    # ~180 B per particle + ~70 B per cell
+    assert 150 * (1 << 20) + 60 * (1 << 21) < out[0] < 260 * (1 << 20) + 90 * (1 << 21)
+    assert out[0] < out[1] < out[2]
