@@ -162,6 +162,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-one-at-a-time comparison")
     ap.add_argument("--workload", default=WORKLOAD)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -301,6 +302,9 @@ def main():
             "gpu_launches": n_launch,
             "clocks": clocks.summary()}
 
+    if not args.no_batched:
+        line["batched"] = batched_comparison(local)
+
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cpu_scene = scenes.WORKLOADS[args.workload](seed=0)
@@ -314,6 +318,76 @@ def main():
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def batched_comparison(local, substeps=200, warmup=20, count=64, seed=0):
+    """The batched workload (scenes.batch_mix: 64 scenes, 200 substeps) run as
+    one batch (one launch per kernel per substep for all scenes, CUDA graph,
+    autotuned launch shape) and one scene at a time through the single-scene
+    path (the same kernels, each scene's `substeps` substeps in turn on its own
+    stream).  Both are device-timed with CUDA events after `warmup` substeps
+    (the autotuner's trials fall in the batch's warm-up)."""
+    import torch
+    from mls_mpm_b200 import abi, scenes
+    from mls_mpm_b200.abi import check
+    from mls_mpm_b200.batch import Batch, default_params
+    from mls_mpm_b200.fluid_gpu import FluidGPU
+
+    mix = scenes.batch_mix(count, seed)
+    n_tot = sum(s.n for s in mix)
+    cells = sum(s.cells for s in mix)
+    dev = torch.device("cuda", local)
+    # batched
+    b = Batch(n_tot, cells, count, device=local, flags=abi.BATCH_AUTOTUNE)
+    for s in mix:
+        b.add(default_params(s.grid, s.n, b.lib), s.pos, s.mass, s.vel, s.affine)
+    b.step(warmup)
+    b.sync()
+    st = torch.cuda.ExternalStream(b.stream(), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.info().launches
+    e0.record(st)
+    b.step(substeps)
+    e1.record(st)
+    e1.synchronize()
+    batched_ms = e0.elapsed_time(e1)
+    info = b.info()
+    launches = info.launches - l0
+    shape = (info.item_blocks, info.grid_blocks)
+    b.close()
+    # one scene at a time
+    alone_ms = 0.0
+    alone_launches = 0
+    for s in mix:
+        fl = FluidGPU.from_scene(s, device=local)
+        lib, h = fl._lib, fl._scene
+        check(lib.mpm_step(h, warmup), "mpm_step")
+        fl.sync()
+        sp = ctypes.c_void_p()
+        check(lib.mpm_get_stream(h, ctypes.byref(sp)), "mpm_get_stream")
+        ss = torch.cuda.ExternalStream(sp.value, device=dev)
+        c0, c1 = ctypes.c_uint64(), ctypes.c_uint64()
+        lib.mpm_launch_count(h, ctypes.byref(c0))
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(ss)
+        check(lib.mpm_step(h, substeps), "mpm_step")
+        a1.record(ss)
+        a1.synchronize()
+        alone_ms += a0.elapsed_time(a1)
+        lib.mpm_launch_count(h, ctypes.byref(c1))
+        alone_launches += c1.value - c0.value
+        fl.destroy()
+    updates = n_tot * substeps
+    sub_bytes = 180 * n_tot + 60 * cells
+    peak, _ = measured_peaks()
+    return {"workload": f"batch_mix: {count} scenes, {n_tot} particles, {cells} cells, seed {seed}",
+            "substeps": substeps, "warmup": warmup,
+            "batched": {"value": updates / (batched_ms / 1e3), "unit": UNIT, "ms_per_substep": batched_ms / substeps,
+                        "gpu_launches": launches, "launch_shape": {"item_blocks": shape[0], "grid_blocks": shape[1]},
+                        "hbm_frac": sub_bytes / (batched_ms / substeps * 1e-3) / 1e9 / peak},
+            "one_at_a_time": {"value": updates / (alone_ms / 1e3), "unit": UNIT,
+                              "ms_per_substep_all_scenes": alone_ms / substeps, "gpu_launches": alone_launches},
+            "speedup": alone_ms / batched_ms}
 
 
 def _profile_traffic(kernel):

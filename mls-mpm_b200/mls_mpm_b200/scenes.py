@@ -17,6 +17,9 @@ Workloads (grid in cells, particle counts exact):
   dam_break_sphere_8m 256x128x256, 8,388,608 particles: a dam block plus a
                      radius-20-cell sphere falling at 2 cells per substep;
                      diffuse pool 1,048,576.
+  batch_mix          64 independent scenes, counts log-uniform in
+                     [4,096, 524,288], cubic grids of edge 32/48/64/96/128,
+                     dam blocks of 20-60% of each axis, 200 substeps.
 """
 import math
 
@@ -138,6 +141,32 @@ def small_box(grid=(24, 20, 22), n=3000, seed=1, lo=(2.0, 2.0, 2.0), counts=None
         nz = -(-n // (nx * ny))
         counts = (nx, ny, nz)
     return dam_break(grid, lo, counts, n, seed, name=name)
+
+
+BATCH_EDGES = (32, 48, 64, 96, 128)
+
+
+def batch_scene(seed, index, n_min=4096, n_max=524288, edges=BATCH_EDGES):
+    """One scene of the batched mix: particle count log-uniform in [n_min,
+    n_max], a cubic grid with edge drawn from `edges`, and a dam block from
+    cell 2 whose extent is U[0.2, 0.6] of each axis, filled with the count at
+    uniform random (seeded) positions — particles per cell = n / block cells,
+    so small blocks with large counts are overpacked."""
+    u = uniform01(seed * 1000003 + index, 5)
+    n = int(round(math.exp(math.log(n_min) + u[0] * (math.log(n_max) - math.log(n_min)))))
+    edge = edges[min(int(u[1] * len(edges)), len(edges) - 1)]
+    ext = [max(1.0, math.floor((0.2 + 0.4 * f) * edge)) for f in u[2:5]]
+    ext = [min(e, edge - 4.0) for e in ext]
+    r = uniform01(seed * 1000003 + index + 7919, 3 * n).reshape(n, 3)
+    pos = (2.0 + r * np.asarray(ext)).astype(np.float32)
+    sc = Scene((edge, edge, edge), pos, name=f"batch_{index}", substeps=200)
+    sc.block_cells = int(ext[0] * ext[1] * ext[2])
+    return sc
+
+
+def batch_mix(count=64, seed=0, **kw):
+    """The batched workload: `count` independent scenes (batch_scene)."""
+    return [batch_scene(seed, i, **kw) for i in range(count)]
 
 
 WORKLOADS = {"dam_break_64": dam_break_64, "dam_break_1m": dam_break_1m,
