@@ -325,6 +325,65 @@ mpm_status mpm_batch_download(mpm_batch* batch, int32_t scene, mpm_buffer which,
 mpm_status mpm_batch_get_stream(mpm_batch* batch, void** stream);
 mpm_status mpm_batch_get_info(mpm_batch* batch, mpm_batch_info* info);
 
+/* ---- serving: a request loop over a batch (no counterpart in the
+ * reference).  Jobs (a scene + a substep count + an arrival time) are queued
+ * with mpm_server_submit; mpm_server_run admits arrived jobs in FIFO order
+ * while they fit the device memory the server was sized for, keeps every
+ * admitted scene resident, advances all active scenes together every
+ * substep, and retires each job after its last substep.  Job latency =
+ * completion (taken in stream order on the device's timeline) - arrival. ---- */
+
+typedef struct mpm_server mpm_server;
+
+/* mpm_server_desc.flags: keep each job's final particle state (pos, vel,
+ * density) on the host for mpm_server_download (costs a synchronous copy per
+ * job; meant for checking results). */
+#define MPM_SERVER_KEEP_STATE 0x100u
+
+typedef struct mpm_server_desc {
+    uint64_t hbm_budget_bytes;     /* device bytes the server's batch may hold */
+    double cells_per_particle;     /* split of the budget between cells and particles (e.g. 2.0) */
+    uint32_t scene_capacity;       /* concurrent scenes */
+    int32_t device;
+    uint32_t flags;                /* MPM_BATCH_* | MPM_SERVER_KEEP_STATE */
+    uint32_t max_inflight;         /* substeps the host may run ahead of the device (0: 2) */
+} mpm_server_desc;
+
+typedef struct mpm_server_stats {
+    uint64_t jobs;                 /* jobs finished */
+    uint64_t substeps;             /* batch substeps run */
+    uint64_t particle_updates;     /* sum over jobs of n * substeps */
+    double wall_s;                 /* from the start of mpm_server_run to the last completion */
+    double p50_latency_s, p99_latency_s, mean_latency_s, max_latency_s;
+    double mean_active, max_active;   /* scenes per batch substep */
+    uint64_t particle_capacity, cell_capacity;   /* what the budget bought */
+    uint64_t launches;             /* kernels launched */
+} mpm_server_stats;
+
+typedef struct mpm_job_result {
+    double arrival_s, admit_s, finish_s;   /* server clock: seconds since mpm_server_run started */
+    uint32_t n, substeps;
+    int32_t done;
+} mpm_job_result;
+
+mpm_status mpm_server_create(const mpm_server_desc* desc, mpm_server** out);
+mpm_status mpm_server_destroy(mpm_server* server);
+
+/* Queues a job.  params: grid dims and uniforms as mpm_set_params takes them
+ * (particle_num replaced by n); host arrays are copied.  MPM_ERR_CAPACITY if
+ * the job can never fit the server. */
+mpm_status mpm_server_submit(mpm_server* server, const mpm_params* params, const float* pos4, const float* vel4,
+                             const float* mass, uint32_t n, uint32_t substeps, double arrival_s, int64_t* job);
+
+/* Runs until every submitted job has finished; fills *stats. */
+mpm_status mpm_server_run(mpm_server* server, mpm_server_stats* stats);
+
+mpm_status mpm_server_job(mpm_server* server, int64_t job, mpm_job_result* out);
+
+/* A finished job's final state (MPM_SERVER_KEEP_STATE): MPM_BUF_POS, VEL or
+ * DENSITY in the reference layout. */
+mpm_status mpm_server_download(mpm_server* server, int64_t job, mpm_buffer which, void* host_dst, size_t bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -198,7 +198,35 @@ SIGNATURES = {
     "mpm_batch_download": (_I, [_V, ctypes.c_int32, _I, _V, _SZ]),
     "mpm_batch_get_stream": (_I, [_V, ctypes.POINTER(_V)]),
     "mpm_batch_get_info": (_I, [_V, _V]),
+    "mpm_server_create": (_I, [_V, ctypes.POINTER(_V)]),
+    "mpm_server_destroy": (_I, [_V]),
+    "mpm_server_submit": (_I, [_V, _V, _V, _V, _V, _U32, _U32, ctypes.c_double, ctypes.POINTER(ctypes.c_int64)]),
+    "mpm_server_run": (_I, [_V, _V]),
+    "mpm_server_job": (_I, [_V, ctypes.c_int64, _V]),
+    "mpm_server_download": (_I, [_V, ctypes.c_int64, _I, _V, _SZ]),
 }
+
+SERVER_KEEP_STATE = 0x100
+
+
+class ServerDesc(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("cells_per_particle", ctypes.c_double),
+                ("scene_capacity", ctypes.c_uint32), ("device", ctypes.c_int32), ("flags", ctypes.c_uint32),
+                ("max_inflight", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("jobs", ctypes.c_uint64), ("substeps", ctypes.c_uint64), ("particle_updates", ctypes.c_uint64),
+                ("wall_s", ctypes.c_double), ("p50_latency_s", ctypes.c_double), ("p99_latency_s", ctypes.c_double),
+                ("mean_latency_s", ctypes.c_double), ("max_latency_s", ctypes.c_double),
+                ("mean_active", ctypes.c_double), ("max_active", ctypes.c_double),
+                ("particle_capacity", ctypes.c_uint64), ("cell_capacity", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64)]
+
+
+class JobResult(ctypes.Structure):
+    _fields_ = [("arrival_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("finish_s", ctypes.c_double),
+                ("n", ctypes.c_uint32), ("substeps", ctypes.c_uint32), ("done", ctypes.c_int32)]
 
 BATCH_NO_GRAPH = 1
 BATCH_AUTOTUNE = 2
