@@ -163,6 +163,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-one-at-a-time comparison")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-vs-per-job comparison")
     ap.add_argument("--workload", default=WORKLOAD)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -304,6 +305,8 @@ def main():
 
     if not args.no_batched:
         line["batched"] = batched_comparison(local)
+    if not args.no_served:
+        line["served"] = served_comparison(local)
 
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -388,6 +391,73 @@ def batched_comparison(local, substeps=200, warmup=20, count=64, seed=0):
             "one_at_a_time": {"value": updates / (alone_ms / 1e3), "unit": UNIT,
                               "ms_per_substep_all_scenes": alone_ms / substeps, "gpu_launches": alone_launches},
             "speedup": alone_ms / batched_ms}
+
+
+def served_comparison(local, rates=(50.0, 200.0, 2000.0), count=64, seed=0, budget_gb=150.0):
+    """The served workload: `count` jobs (scenes.serve_job) arriving as a
+    Poisson stream at each rate, run by the serving loop (admission against an
+    HBM budget, resident scenes batched every substep) and by the plain
+    per-job path (one job at a time in arrival order through the single-scene
+    path).  Plain-path latencies come from each job's device-timed service
+    time played through the same arrival times in FIFO order."""
+    import torch
+    from mls_mpm_b200 import abi, scenes
+    from mls_mpm_b200.abi import check
+    from mls_mpm_b200.batch import default_params
+    from mls_mpm_b200.fluid_gpu import FluidGPU
+    from mls_mpm_b200.server import Server
+
+    jobs = [scenes.serve_job(seed, i) for i in range(count)]
+    updates = sum(sc.n * k for sc, k in jobs)
+    dev = torch.device("cuda", local)
+    free, _ = torch.cuda.mem_get_info(dev)
+    budget = int(min(budget_gb * 1e9, free - 12e9))
+    cpp = max(sc.cells / sc.n for sc, _ in jobs)
+    out = {"workload": f"serve_job x{count}: {sum(sc.n for sc, _ in jobs)} particles, "
+                       f"{updates} particle-updates, seed {seed}",
+           "budget_bytes": budget, "budget_note": f"min({budget_gb:g} GB, free device memory - 12 GB)",
+           "rates": {}}
+    # plain per-job path: service time of each job alone (device-timed)
+    service = []
+    for sc, k in jobs:
+        fl = FluidGPU.from_scene(sc, device=local)
+        lib, h = fl._lib, fl._scene
+        sp = ctypes.c_void_p()
+        check(lib.mpm_get_stream(h, ctypes.byref(sp)), "mpm_get_stream")
+        ss = torch.cuda.ExternalStream(sp.value, device=dev)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(ss)
+        check(lib.mpm_step(h, k), "mpm_step")
+        a1.record(ss)
+        a1.synchronize()
+        service.append(a0.elapsed_time(a1) / 1e3)
+        fl.destroy()
+    srv = Server(budget, scene_capacity=max(64, count), cells_per_particle=cpp, device=local)
+    try:
+        for rate in rates:
+            arr = scenes.poisson_arrivals(rate, count, seed)
+            for (sc, k), t in zip(jobs, arr):
+                srv.submit(default_params(sc.grid, sc.n, srv.lib), sc.pos, sc.mass, k, float(t), vel4=sc.vel)
+            st = srv.run()
+            # plain path, FIFO through the same arrivals
+            fin, lat = 0.0, []
+            for t, sv in zip(arr, service):
+                fin = max(fin, t) + sv
+                lat.append(fin - t)
+            out["rates"][f"{rate:g}"] = {
+                "served": {"value": st.particle_updates / st.wall_s, "unit": UNIT,
+                           "p50_latency_s": st.p50_latency_s, "p99_latency_s": st.p99_latency_s,
+                           "wall_s": st.wall_s, "mean_active_scenes": st.mean_active,
+                           "max_active_scenes": st.max_active, "substeps": st.substeps,
+                           "gpu_launches": st.launches},
+                "plain_per_job": {"value": updates / fin, "unit": UNIT,
+                                  "p50_latency_s": float(np.percentile(lat, 50)),
+                                  "p99_latency_s": float(np.percentile(lat, 99)), "wall_s": fin},
+                "speedup": (st.particle_updates / st.wall_s) / (updates / fin)}
+        out["capacity"] = {"particles": st.particle_capacity, "cells": st.cell_capacity}
+    finally:
+        srv.close()
+    return out
 
 
 def _profile_traffic(kernel):

@@ -375,7 +375,8 @@ mpm_status mpm_server_destroy(mpm_server* server);
 mpm_status mpm_server_submit(mpm_server* server, const mpm_params* params, const float* pos4, const float* vel4,
                              const float* mass, uint32_t n, uint32_t substeps, double arrival_s, int64_t* job);
 
-/* Runs until every submitted job has finished; fills *stats. */
+/* Runs until every job submitted since the last run has finished (the clock
+ * restarts at 0 for each run); fills *stats for those jobs. */
 mpm_status mpm_server_run(mpm_server* server, mpm_server_stats* stats);
 
 mpm_status mpm_server_job(mpm_server* server, int64_t job, mpm_job_result* out);

@@ -172,6 +172,7 @@ mpm_status mpm_server_run(mpm_server* s, mpm_server_stats* stats) {
     std::deque<Job*> queue;
     for (auto& j : s->jobs)
         if (j->state == 0) queue.push_back(j.get());
+    const std::vector<Job*> this_run(queue.begin(), queue.end());   // stats cover the jobs of this call
     std::stable_sort(queue.begin(), queue.end(), [](const Job* a, const Job* b) { return a->arrival < b->arrival; });
     const size_t R = s->max_inflight + 1;
     std::vector<cudaEvent_t> ev(R, nullptr);
@@ -259,7 +260,7 @@ mpm_status mpm_server_run(mpm_server* s, mpm_server_stats* stats) {
         std::memset(stats, 0, sizeof *stats);
         std::vector<double> lat;
         double last = 0.0;
-        for (auto& j : s->jobs) {
+        for (Job* j : this_run) {
             if (j->state != 2) continue;
             lat.push_back(j->finish - j->arrival);
             last = std::max(last, (double)j->finish);

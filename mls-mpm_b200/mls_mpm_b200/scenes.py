@@ -20,6 +20,9 @@ Workloads (grid in cells, particle counts exact):
   batch_mix          64 independent scenes, counts log-uniform in
                      [4,096, 524,288], cubic grids of edge 32/48/64/96/128,
                      dam blocks of 20-60% of each axis, 200 substeps.
+  serve_job          served jobs: counts log-uniform in [8,192, 2,097,152],
+                     grid edge 32-192 at 8 particles per cell in the dam
+                     block, 50-500 substeps; Poisson arrivals.
 """
 import math
 
@@ -167,6 +170,32 @@ def batch_scene(seed, index, n_min=4096, n_max=524288, edges=BATCH_EDGES):
 def batch_mix(count=64, seed=0, **kw):
     """The batched workload: `count` independent scenes (batch_scene)."""
     return [batch_scene(seed, i, **kw) for i in range(count)]
+
+
+def serve_job(seed, index, n_min=8192, n_max=2097152, steps_min=50, steps_max=500):
+    """One job of the served workload: particle count log-uniform in [n_min,
+    n_max]; a cubic grid whose edge (32..192, a multiple of 8) makes a dam
+    block of 40% x 60% x 40% of the domain hold the particles at 8 per cell
+    (2 x 2 x 2 lattice, jitter +-0.25 cell); substeps uniform in
+    [steps_min, steps_max].  Returns (scene, substeps)."""
+    u = uniform01(seed * 1000033 + index, 2)
+    n = int(round(math.exp(math.log(n_min) + u[0] * (math.log(n_max) - math.log(n_min)))))
+    edge = int(math.ceil((n / (8 * 0.4 * 0.6 * 0.4)) ** (1.0 / 3.0) / 8.0) * 8)
+    edge = min(192, max(32, edge))
+    nx = int(0.4 * edge / 0.5)
+    ny = int(0.6 * edge / 0.5)
+    nz = -(-n // (nx * ny))
+    sc = dam_break((edge, edge, edge), (2.0, 2.0, 2.0), (nx, ny, nz), n, seed * 7919 + index,
+                   name=f"job_{index}")
+    steps = steps_min + min(int(u[1] * (steps_max - steps_min + 1)), steps_max - steps_min)
+    return sc, steps
+
+
+def poisson_arrivals(rate, count, seed):
+    """Arrival times (s) of a Poisson process of `rate` jobs/s."""
+    u = uniform01(seed * 1000037 + 17, count)
+    gaps = -np.log1p(-u) / rate
+    return np.cumsum(gaps) - gaps[0]
 
 
 WORKLOADS = {"dam_break_64": dam_break_64, "dam_break_1m": dam_break_1m,
