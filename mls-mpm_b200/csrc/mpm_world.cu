@@ -1,30 +1,32 @@
-// mpm_world.cu — the binned, item-major MLS-MPM substep over a world of scenes.
+// mpm_world.cu — the binned MLS-MPM substep over a world of scenes.
 //
 // Same arithmetic as mpm_kernels.cu (and so the same bits), organised for
 // the B200:
-//   * Work item = up to kMaxL particles of one cell.  One thread owns an
-//     item: the 27 neighbour masses (P2G_MOM) or velocities (G2P) are loaded
-//     once per item, and P2G contributions are summed as i32 (the same
-//     wrapping sums the reference's atomics produce), flushed with one
-//     atomic per (cell, component) per item.
-//   * Items are bucketed by length, and particles are stored warp-interleaved:
-//     the k-th particle of the item held by lane l of warp w of bucket b sits
-//     at position pos_off[b] + w*32*b + k*32 + l.  All 32 lanes of a warp run
-//     the same trip count and every per-particle load/store is coalesced.
-//   * Within a bucket, items are ordered by (tile, cell) — a deterministic
-//     layout that changes little from one substep to the next, so reading a
-//     particle through the permutation (new position -> previous position)
-//     stays nearly coalesced.  Cells holding more than kMaxL particles are
-//     split into several items placed after the ordered ones.
+//   * Particles are sorted by (tile, cell) every substep (counting sort:
+//     per-cell ranks, a scan per 16x8x8-cell tile, a two-level scan over
+//     tiles) and each tile's particles are cut into chunks of up to kChunk
+//     consecutive particles.  The new layout reads the previous one through
+//     a permutation (new position -> previous position), which stays nearly
+//     coalesced because the order changes little between substeps.
+//   * P2G_MASS, P2G_MOM and G2P run one block per chunk, one thread per
+//     particle.  A chunk's cells form a box inside its tile; P2G sums the
+//     i32 contributions of the box plus a one-cell halo in shared memory —
+//     lanes whose particles share a cell first add their values with one
+//     warp reduction (integer adds commute, so the bits equal the
+//     reference's atomics) — and flushes each halo cell to the grid with one
+//     atomic.  G2P stages the halo's grid velocities in shared memory and
+//     gathers from there.  Particles whose stencil leaves the halo or the
+//     grid take a direct path with the reference's own indexing.
 //   * Scenes: cells, tiles and particle ids of every scene are ranges of the
-//     world's arrays; an item carries its scene, a tile maps to its scene,
-//     and each kernel reads the scene's grid dims, params and walls from the
-//     device scene table.  All scenes advance in one launch per kernel.
-//   * The grid is processed per tile (16x8x8 cells) and only for tiles a
-//     particle stencil touches now or touched last substep (cells elsewhere
-//     are zero, as the reference's CLEAR/DECODE/UPDATE would leave them).
-//     The i32 grid is double-buffered: UPDATE_GRID of substep s reads
-//     buffer s%2 and zeroes buffer (s+1)%2, which is the CLEAR of s+1.
+//     world's arrays; a tile maps to its scene, and each kernel reads the
+//     scene's grid dims, params, walls and hand from the device scene table.
+//     All scenes advance in one launch per kernel.
+//   * The grid is processed per tile and only for tiles a particle stencil
+//     touches now or touched last substep (cells elsewhere are zero, as the
+//     reference's CLEAR/DECODE/UPDATE would leave them).  The i32 grid is
+//     double-buffered: UPDATE_GRID of substep s reads buffer s%2 and zeroes
+//     buffer (s+1)%2, which is the CLEAR of s+1.  APPLY_HAND runs inside the
+//     UPDATE_GRID pass.
 //   * The diffuse spawn decision runs in the G2P epilogue (post-G2P pos/vel,
 //     this substep's density), staging records by particle id.
 #include <cuda_runtime.h>
@@ -83,31 +85,23 @@ WorldView World::view() const {
     WorldView v;
     v.npos = npos;
     v.ntiles = (uint32_t)tiles.high_water();
-    v.nchunks = (v.ntiles + 1023u) / 1024u;
-    if (v.nchunks == 0) v.nchunks = 1;
-    for (int b = 0; b < kMaxL + 2; ++b) v.cap_off[b] = cap_off[b];
+    v.ngroups = (v.ntiles + 1023u) / 1024u;
+    if (v.ngroups == 0) v.ngroups = 1;
+    v.chunk_cap = chunk_cap;
     v.scenes = d_scenes;
     v.tile_scene = tile_scene;
-    v.cell_count = cell_count; v.cell_info = cell_info; v.bucket_items = bucket_items;
+    v.cell_count = cell_count; v.cell_start = cell_start;
     v.key = key; v.rank = rank; v.perm = perm;
-    v.tile_flags = tile_flags; v.tile_occ = tile_occ; v.tile_hist = tile_hist; v.tile_base_ = tile_base;
-    v.tile_occ_list = tile_occ_list; v.tile_grid_list = tile_grid_list; v.tile_chunk = tile_chunk;
+    v.tile_flags = tile_flags; v.tile_occ = tile_occ; v.tile_cnt = tile_cnt;
+    v.tile_pstart = tile_pstart; v.tile_cstart = tile_cstart;
+    v.group_pstart = group_pstart; v.group_cstart = group_cstart;
+    v.chunk_info = chunk_info; v.chunk_last = chunk_last;
+    v.tile_occ_list = tile_occ_list; v.tile_grid_list = tile_grid_list;
     v.ctrl = ctrl; v.dens = dens;
     return v;
 }
 
 namespace {
-
-constexpr int kItemThreads = 128;
-
-// Register-pressure strategies of the item kernels (compile-time; defaults
-// are the measured best: see the profiles for the A/B).
-#ifndef MPM_MOM_LB
-#define MPM_MOM_LB 1
-#endif
-#ifndef MPM_G2P_LB
-#define MPM_G2P_LB 3
-#endif
 
 __device__ __forceinline__ int32_t clampi(int32_t v, int32_t lo, int32_t hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -206,7 +200,7 @@ __global__ void k_set_total(Ctrl* ctrl, uint32_t total) {
 }
 
 // ---------------------------------------------------------------------------
-// Binning
+// Binning: particles sorted by (tile, cell), tiles cut into chunks
 // ---------------------------------------------------------------------------
 
 // Rank of every particle of the current state within its binning cell.
@@ -229,17 +223,44 @@ __global__ void k_tiles_occ(WorldView v) {
     if (occ) v.tile_occ_list[atomicAdd(&v.ctrl->n_occ, 1u)] = t;
 }
 
-// One block per occupied tile, one thread per cell.  A cell with 1..kMaxL
-// particles becomes one item in bucket `count`, ranked within the tile by
-// cell index (match + warp prefix); the tile's per-bucket totals go to
-// tile_hist.  Larger cells are split into items that take unordered slots
-// after the ordered ones.  Also marks every tile the particles' 3x3x3
-// stencils touch (bit 1) and clears the counts.
+
+__device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t x, uint32_t* ws, uint32_t& total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t sc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, sc, o);
+        if (lane >= o) sc += y;
+    }
+    if (lane == 31) ws[wid] = sc;
+    __syncthreads();
+    if (wid == 0) {
+        const uint32_t w = ws[lane];
+        uint32_t ww = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, ww, o);
+            if (lane >= o) ww += y;
+        }
+        ws[lane] = ww - w;
+        if (lane == 31) ws[32] = ww;
+    }
+    __syncthreads();
+    const uint32_t r = ws[wid] + sc - x;
+    total = ws[32];
+    __syncthreads();
+    return r;
+}
+
+
+// One block per occupied tile, one thread per cell (local order x fastest,
+// then y, then z): exclusive scan of the cell counts inside the tile ->
+// cell_start (tile-local), tile total -> tile_cnt.  Also marks every tile the
+// particles' 3x3x3 stencils touch (bit 1).
 __global__ void __launch_bounds__(kTileCells) k_bin_cells(WorldView v) {
-    __shared__ uint32_t wcnt[kTileCells / 32][kMaxL + 1];
+    __shared__ uint32_t ws[33];
     __shared__ uint32_t dirs;
     const uint32_t nocc = v.ctrl->n_occ;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (uint32_t ti = blockIdx.x; ti < nocc; ti += gridDim.x) {
         const uint32_t t = v.tile_occ_list[ti];
         const uint32_t scene = v.tile_scene[t];
@@ -251,13 +272,8 @@ __global__ void __launch_bounds__(kTileCells) k_bin_cells(WorldView v) {
         const uint32_t x = tx * kTileX + lx, y = ty * kTileY + ly, z = tz * kTileZ + lz;
         const bool inside = x < sd.X && y < sd.Y && z < sd.Z;
         const uint32_t c = inside ? sd.cell_base + local_cell(sd, x, y, z) : 0u;
-        uint32_t cnt = 0;
-        if (inside) {
-            cnt = v.cell_count[c];
-            if (cnt) v.cell_count[c] = 0u;
-        }
+        const uint32_t cnt = inside ? v.cell_count[c] : 0u;
         if (threadIdx.x == 0) dirs = 0u;
-        for (int b = lane; b <= kMaxL; b += 32) wcnt[wid][b] = 0u;
         __syncthreads();
         // neighbour tiles this cell's stencil reaches (3x3x3 direction bits)
         uint32_t m = 0;
@@ -271,22 +287,11 @@ __global__ void __launch_bounds__(kTileCells) k_bin_cells(WorldView v) {
                         m |= 1u << ((kz * dz + 1) * 9 + (ky * dy + 1) * 3 + (kx * dx + 1));
         }
         const uint32_t wm = __reduce_or_sync(0xffffffffu, m);
-        if (lane == 0 && wm) atomicOr(&dirs, wm);
-        const uint32_t b = (cnt >= 1 && cnt <= (uint32_t)kMaxL) ? cnt : 0u;
-        const uint32_t grp = __match_any_sync(0xffffffffu, b);
-        const uint32_t lrank = __popc(grp & ((1u << lane) - 1u));
-        if (b && lrank == 0) wcnt[wid][b] = __popc(grp);
-        __syncthreads();
-        // exclusive prefix over the 32 warps for each length; tile totals
-        if (threadIdx.x >= 1 && threadIdx.x <= kMaxL) {
-            uint32_t acc = 0;
-            for (int w = 0; w < kTileCells / 32; ++w) {
-                const uint32_t k = wcnt[w][threadIdx.x];
-                wcnt[w][threadIdx.x] = acc;
-                acc += k;
-            }
-            v.tile_hist[(size_t)(threadIdx.x - 1) * v.ntiles + t] = acc;
-        }
+        if ((threadIdx.x & 31) == 0 && wm) atomicOr(&dirs, wm);
+        uint32_t total;
+        const uint32_t local = block_exclusive_scan_1024(cnt, ws, total);   // also orders the dirs updates
+        if (cnt) v.cell_start[c] = local;
+        if (threadIdx.x == 0) v.tile_cnt[t] = total;
         if (threadIdx.x < 27 && ((dirs >> threadIdx.x) & 1u)) {
             const int ox = (int)(threadIdx.x % 3) - 1, oy = (int)((threadIdx.x / 3) % 3) - 1,
                       oz = (int)(threadIdx.x / 9) - 1;
@@ -295,19 +300,6 @@ __global__ void __launch_bounds__(kTileCells) k_bin_cells(WorldView v) {
                 const uint32_t nt = sd.tile_base + ((uint32_t)nz * sd.nty + (uint32_t)ny) * sd.ntx + (uint32_t)nx;
                 if ((v.tile_flags[nt] & 2u) == 0u) atomicOr(&v.tile_flags[nt], 2u);
             }
-        }
-        __syncthreads();
-        if (b) {
-            v.cell_info[c] = make_uint4(b | (b << 8) | (1u << 16), wcnt[wid][b] + lrank, t, scene);
-        } else if (cnt) {
-            // overpacked cell: q items of length L (the last of Llast), unordered tail slots
-            const uint32_t q = (cnt + kMaxL - 1) / kMaxL;
-            const uint32_t L = (cnt + q - 1) / q;
-            const uint32_t Llast = cnt - (q - 1) * L;
-            const uint32_t nL = (Llast == L) ? q : q - 1;
-            const uint32_t idxL = atomicAdd(&v.ctrl->tail_cnt[L], nL);
-            const uint32_t idxLast = (Llast != L) ? atomicAdd(&v.ctrl->tail_cnt[Llast], 1u) : idxL + q - 1;
-            v.cell_info[c] = make_uint4(L | (Llast << 8) | (q << 16) | 0x80000000u, idxL, idxLast, scene);
         }
         __syncthreads();
     }
@@ -339,170 +331,101 @@ __global__ void k_tiles_grid(WorldView v) {
     if (f != (now ? 4u : 0u)) v.tile_flags[t] = now ? 4u : 0u;
 }
 
-// Exclusive scan of the ordered item counts of each length bucket over all
-// tiles in index order, in two levels.  Level 1, one block per (1024-tile
-// chunk, bucket): tile_base = prefix inside the chunk, tile_chunk = chunk total.
-__device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t x, uint32_t* ws, uint32_t& total) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t sc = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, sc, o);
-        if (lane >= o) sc += y;
-    }
-    if (lane == 31) ws[wid] = sc;
-    __syncthreads();
-    if (wid == 0) {
-        const uint32_t w = ws[lane];
-        uint32_t ww = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, ww, o);
-            if (lane >= o) ww += y;
-        }
-        ws[lane] = ww - w;
-        if (lane == 31) ws[32] = ww;
-    }
-    __syncthreads();
-    const uint32_t r = ws[wid] + sc - x;
-    total = ws[32];
-    __syncthreads();
-    return r;
-}
 
+// Two-level exclusive scan over all tiles in index order of the particle
+// counts and the chunk counts of the occupied tiles.  Level 1, one block per
+// group of 1024 tiles: prefixes inside the group, group totals.
 __global__ void __launch_bounds__(1024) k_tile_scan_local(WorldView v) {
     __shared__ uint32_t ws[33];
-    const uint32_t chunk = blockIdx.x, b = blockIdx.y;
-    const uint32_t t = chunk * 1024u + threadIdx.x;
-    const uint32_t x = (t < v.ntiles && v.tile_occ[t]) ? v.tile_hist[(size_t)b * v.ntiles + t] : 0u;
-    uint32_t total;
-    const uint32_t r = block_exclusive_scan_1024(x, ws, total);
-    if (t < v.ntiles) v.tile_base_[(size_t)b * v.ntiles + t] = r;
-    if (threadIdx.x == 0) v.tile_chunk[(size_t)b * v.nchunks + chunk] = total;
+    const uint32_t g = blockIdx.x;
+    const uint32_t t = g * 1024u + threadIdx.x;
+    const uint32_t np = (t < v.ntiles && v.tile_occ[t]) ? v.tile_cnt[t] : 0u;
+    const uint32_t nc = (np + kChunk - 1) / kChunk;
+    uint32_t tp, tc;
+    const uint32_t rp = block_exclusive_scan_1024(np, ws, tp);
+    const uint32_t rc = block_exclusive_scan_1024(nc, ws, tc);
+    if (t < v.ntiles) {
+        v.tile_pstart[t] = rp;
+        v.tile_cstart[t] = rc;
+    }
+    if (threadIdx.x == 0) {
+        v.group_pstart[g] = tp;
+        v.group_cstart[g] = tc;
+    }
 }
 
-// Level 2, one block per bucket: exclusive scan of the chunk totals in place;
-// the bucket total goes to bucket_reg.
-__global__ void __launch_bounds__(1024) k_tile_scan_chunks(WorldView v) {
+// Level 2, one block: exclusive scan of the group totals; the layout size and
+// chunk count go to ctrl.  Also advances the diffuse seed (diffuse-gpu.js:149).
+__global__ void __launch_bounds__(1024) k_tile_scan_top(WorldView v, mpm_gen_params* gen) {
     __shared__ uint32_t ws[33];
-    const uint32_t b = blockIdx.x;
-    uint32_t* chunks = v.tile_chunk + (size_t)b * v.nchunks;
-    uint32_t carry = 0;
-    for (uint32_t c0 = 0; c0 < v.nchunks; c0 += 1024) {
-        const uint32_t c = c0 + threadIdx.x;
-        const uint32_t x = c < v.nchunks ? chunks[c] : 0u;
-        uint32_t total;
-        const uint32_t r = block_exclusive_scan_1024(x, ws, total);
-        if (c < v.nchunks) chunks[c] = carry + r;
-        carry += total;
+    uint32_t cp = 0, cc = 0;
+    for (uint32_t g0 = 0; g0 < v.ngroups; g0 += 1024) {
+        const uint32_t g = g0 + threadIdx.x;
+        const uint32_t xp = g < v.ngroups ? v.group_pstart[g] : 0u;
+        const uint32_t xc = g < v.ngroups ? v.group_cstart[g] : 0u;
+        uint32_t tp, tc;
+        const uint32_t rp = block_exclusive_scan_1024(xp, ws, tp);
+        const uint32_t rc = block_exclusive_scan_1024(xc, ws, tc);
+        if (g < v.ngroups) {
+            v.group_pstart[g] = cp + rp;
+            v.group_cstart[g] = cc + rc;
+        }
+        cp += tp;
+        cc += tc;
     }
-    if (threadIdx.x == 0) v.ctrl->bucket_reg[b + 1] = carry;
-}
-
-// Bucket offsets (one warp): ordered + tail items, padded to whole warps.
-// Also advances the diffuse seed (diffuse-gpu.js:149) for this substep.
-__global__ void k_bucket_scan(Ctrl* ctrl, mpm_gen_params* gen) {
-    const int lane = threadIdx.x;
-    const uint32_t b = (uint32_t)lane;
-    const uint32_t cnt = (b >= 1 && b <= (uint32_t)kMaxL) ? ctrl->bucket_reg[b] + ctrl->tail_cnt[b] : 0u;
-    const uint32_t pad = (cnt + 31u) & ~31u;
-    uint32_t si = pad, sp = pad * b;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t yi = __shfl_up_sync(0xffffffffu, si, o);
-        const uint32_t yp = __shfl_up_sync(0xffffffffu, sp, o);
-        if (lane >= o) { si += yi; sp += yp; }
-    }
-    if (b <= (uint32_t)kMaxL + 1) {
-        ctrl->item_off[b] = si - pad;
-        ctrl->pos_off[b] = sp - pad * b;
-        ctrl->bucket_cnt[b] = cnt;
-    }
-    const uint32_t ti = __shfl_sync(0xffffffffu, si, kMaxL);
-    const uint32_t tp = __shfl_sync(0xffffffffu, sp, kMaxL);
-    if (lane == 0) {
-        ctrl->total_items = ti;
-        ctrl->prev_total_pos = ctrl->total_pos;
-        ctrl->total_pos = tp;
+    if (threadIdx.x == 0) {
+        v.ctrl->prev_total_pos = v.ctrl->total_pos;
+        v.ctrl->total_pos = min(cp, v.npos);
+        v.ctrl->total_chunks = min(cc, v.chunk_cap);
         if (gen) gen->seed = gen->seed + 1u;
     }
 }
 
-__device__ __forceinline__ uint32_t item_position(const uint32_t* pos_off, uint32_t b, uint32_t idx) {
-    return pos_off[b] + (idx >> 5) * 32u * b + (idx & 31u);
+// One block per occupied tile, one thread per cell: cell_start becomes the
+// global first position, the counts are cleared, and the tile's chunks are
+// written: (tile, first position, end position, first local cell) and the
+// last local cell, each by the thread whose cell holds that particle.
+__global__ void __launch_bounds__(kTileCells) k_tile_finish(WorldView v) {
+    const uint32_t nocc = v.ctrl->n_occ;
+    for (uint32_t ti = blockIdx.x; ti < nocc; ti += gridDim.x) {
+        const uint32_t t = v.tile_occ_list[ti];
+        const uint32_t scene = v.tile_scene[t];
+        const SceneDesc& sd = v.scenes[scene];
+        const uint32_t lt = t - sd.tile_base;
+        const uint32_t tx = lt % sd.ntx, ty = (lt / sd.ntx) % sd.nty, tz = lt / (sd.ntx * sd.nty);
+        const uint32_t lid = threadIdx.x;
+        const uint32_t x = tx * kTileX + lid % kTileX, y = ty * kTileY + (lid / kTileX) % kTileY,
+                       z = tz * kTileZ + lid / (kTileX * kTileY);
+        if (x >= sd.X || y >= sd.Y || z >= sd.Z) continue;
+        const uint32_t c = sd.cell_base + local_cell(sd, x, y, z);
+        const uint32_t cnt = v.cell_count[c];
+        if (cnt == 0) continue;
+        const uint32_t base_p = v.tile_pstart[t] + v.group_pstart[t >> 10];
+        const uint32_t base_c = v.tile_cstart[t] + v.group_cstart[t >> 10];
+        const uint32_t total = v.tile_cnt[t];
+        const uint32_t a = v.cell_start[c];
+        v.cell_start[c] = base_p + a;
+        v.cell_count[c] = 0u;
+        for (uint32_t j = a / kChunk; j <= (a + cnt - 1) / kChunk; ++j) {
+            const uint32_t ci = base_c + j;
+            if (ci >= v.chunk_cap) break;
+            const uint32_t f = j * kChunk;
+            const uint32_t e = min(f + kChunk, total);
+            if (f >= a) v.chunk_info[ci] = make_uint4(t, base_p + f, base_p + e, lid);
+            if (e - 1 < a + cnt) v.chunk_last[ci] = lid;
+        }
+    }
 }
 
-// perm[new position] = previous position for every particle; the first
-// particle of each item also records the item's (cell, scene).
+// perm[new position] = previous position for every particle.
 __global__ void k_scatter(WorldView v) {
-    __shared__ uint32_t pos_off[kMaxL + 2];
-    __shared__ uint32_t reg[kMaxL + 2];
-    if (threadIdx.x < kMaxL + 2) {
-        pos_off[threadIdx.x] = v.ctrl->pos_off[threadIdx.x];
-        reg[threadIdx.x] = v.ctrl->bucket_reg[threadIdx.x];
-    }
-    __syncthreads();
     const uint32_t total = v.ctrl->prev_total_pos;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const uint32_t c = v.key[i];
         if (c == kHole) continue;
-        const uint32_t r = v.rank[i];
-        const uint4 info = v.cell_info[c];
-        uint32_t b, idx, kk;
-        if (!(info.x & 0x80000000u)) {
-            b = info.x & 0xFFu;
-            const size_t row = (size_t)(b - 1);
-            idx = v.tile_base_[row * v.ntiles + info.z] + v.tile_chunk[row * v.nchunks + (info.z >> 10)] + info.y;
-            kk = r;
-        } else {
-            const uint32_t L = info.x & 0xFFu, Llast = (info.x >> 8) & 0xFFu, q = (info.x >> 16) & 0x7FFFu;
-            const uint32_t it = r / L;
-            kk = r - it * L;
-            if (it + 1 < q || Llast == L) { b = L; idx = reg[L] + info.y + it; }
-            else { b = Llast; idx = reg[Llast] + info.z; }
-        }
-        if (b < 1 || b > (uint32_t)kMaxL) continue;
-        const uint32_t pos = item_position(pos_off, b, idx) + kk * 32u;
-        if (pos >= v.npos) continue;
-        v.perm[pos] = i;
-        if (kk == 0 && v.cap_off[b] + idx < v.cap_off[b + 1])
-            v.bucket_items[v.cap_off[b] + idx] = make_uint2(c, info.w);
+        const uint32_t pos = v.cell_start[c] + v.rank[i];
+        if (pos < v.npos) v.perm[pos] = i;
     }
-}
-
-// Shared copy of the bucket tables for the item kernels.
-struct ItemTables {
-    uint32_t item_off[kMaxL + 2];
-    uint32_t pos_off[kMaxL + 2];
-    uint32_t cnt[kMaxL + 2];
-};
-
-__device__ __forceinline__ void load_tables(const WorldView& v, ItemTables& t) {
-    if (threadIdx.x < kMaxL + 2) {
-        t.item_off[threadIdx.x] = v.ctrl->item_off[threadIdx.x];
-        t.pos_off[threadIdx.x] = v.ctrl->pos_off[threadIdx.x];
-        t.cnt[threadIdx.x] = (threadIdx.x >= 1 && threadIdx.x <= kMaxL) ? v.ctrl->bucket_cnt[threadIdx.x] : 0u;
-    }
-    __syncthreads();
-}
-
-struct ItemRef {
-    uint32_t b, idx, cell, scene, pbase;
-    bool valid;
-};
-
-__device__ __forceinline__ ItemRef item_ref(const WorldView& v, const ItemTables& t, uint32_t g) {
-    ItemRef r;
-    uint32_t b = 1;
-    while (b < (uint32_t)kMaxL && g >= t.item_off[b + 1]) ++b;
-    r.b = b;
-    r.idx = g - t.item_off[b];
-    r.valid = r.idx < t.cnt[b];
-    const uint2 e = r.valid ? v.bucket_items[v.cap_off[b] + r.idx] : make_uint2(0u, 0u);
-    r.cell = e.x;
-    r.scene = e.y;
-    r.pbase = item_position(t.pos_off, b, r.idx);
-    return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -535,80 +458,185 @@ __device__ __forceinline__ void cell_xyz(const SceneDesc& sd, uint32_t gc, int32
 // encode() without the clamp, for values already known to lie in +-20000.
 __device__ __forceinline__ int32_t encode_unclamped(float v) { return __float2int_rz(v * kFixed); }
 
+
 // ---------------------------------------------------------------------------
-// P2G_MASS (shaders.js:242-274), item-major
+// Chunks: the halo box of a chunk's cells in shared memory
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kItemThreads) k_p2g_mass_items(WorldView v, const float4* __restrict__ posm,
-                                                                 int32_t* __restrict__ cm) {
-    __shared__ ItemTables tabs;
-    load_tables(v, tabs);
-    const uint32_t nitems = v.ctrl->total_items;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nitems; g += gridDim.x * blockDim.x) {
-        const ItemRef it = item_ref(v, tabs, g);
-        if (!it.valid) continue;
-        const SceneDesc& sd = v.scenes[it.scene];
-        const int32_t X = sd.X, Y = sd.Y, Z = sd.Z;
-        int32_t* scm = cm + sd.cell_base;
-        int32_t ix, iy, iz;
-        cell_xyz(sd, it.cell, ix, iy, iz);
-        int32_t acc[27];
+// Shared-memory accumulation strategy of the P2G chunk kernels:
+//   MPM_P2G_AGG 1: lanes with the same stencil add their values with one warp
+//                  reduction, one lane adds the sum; 0: every lane adds its own.
+//   MPM_P2G_SPREAD 1: within each pass over the chunk, lane l of warp w takes
+//                  particle 8*l + w (neighbouring lanes in different cells, so
+//                  the lanes of one shared atomic rarely share an address);
+//                  0: lane order = particle order.
+#ifndef MPM_P2G_AGG
+#define MPM_P2G_AGG 0
+#endif
+#ifndef MPM_P2G_SPREAD
+#define MPM_P2G_SPREAD 1
+#endif
+
+__device__ __forceinline__ uint32_t chunk_lane_offset() {
+#if MPM_P2G_SPREAD
+    return (threadIdx.x & 31u) * (kChunkThreads / 32) + (threadIdx.x >> 5);
+#else
+    return threadIdx.x;
+#endif
+}
+
+struct ChunkHdr {
+    uint32_t scene, first, end;
+    int32_t ox, oy, oz;      // scene-local cell at halo index 0
+    int32_t hx, hy, hz;      // halo dims
+};
+
+// The box of the local cells [lo, hi] (x fastest, then y, then z) plus one
+// cell on every side.
+__device__ __forceinline__ void chunk_header(const WorldView& v, uint32_t ch, ChunkHdr& h) {
+    const uint4 ci = v.chunk_info[ch];
+    const uint32_t lo = ci.w, hi = v.chunk_last[ch];
+    const uint32_t t = ci.x;
+    const uint32_t scene = v.tile_scene[t];
+    const SceneDesc& sd = v.scenes[scene];
+    const uint32_t lt = t - sd.tile_base;
+    const int32_t tx = (int32_t)(lt % sd.ntx), ty = (int32_t)((lt / sd.ntx) % sd.nty),
+                  tz = (int32_t)(lt / (sd.ntx * sd.nty));
+    constexpr uint32_t kRow = kTileX, kSlab = kTileX * kTileY;
+    int32_t x0 = 0, x1 = kTileX - 1, y0 = 0, y1 = kTileY - 1;
+    const int32_t z0 = (int32_t)(lo / kSlab), z1 = (int32_t)(hi / kSlab);
+    if (z0 == z1) {
+        y0 = (int32_t)((lo / kRow) % kTileY);
+        y1 = (int32_t)((hi / kRow) % kTileY);
+        if (y0 == y1) {
+            x0 = (int32_t)(lo % kRow);
+            x1 = (int32_t)(hi % kRow);
+        }
+    }
+    h.scene = scene;
+    h.first = ci.y;
+    h.end = ci.z;
+    h.ox = tx * kTileX + x0 - 1;
+    h.oy = ty * kTileY + y0 - 1;
+    h.oz = tz * kTileZ + z0 - 1;
+    h.hx = x1 - x0 + 3;
+    h.hy = y1 - y0 + 3;
+    h.hz = z1 - z0 + 3;
+}
+
+// True when the particle's 3x3x3 stencil lies in the chunk's halo box and in
+// the grid (then shared-memory accumulation / gathering is exact); otherwise
+// the particle takes the direct path with the reference's indexing.
+__device__ __forceinline__ bool in_halo(const PW& w, const ChunkHdr& h, const SceneDesc& sd) {
+    return w.cx - 1 >= h.ox && w.cy - 1 >= h.oy && w.cz - 1 >= h.oz && w.cx + 1 < h.ox + h.hx &&
+           w.cy + 1 < h.oy + h.hy && w.cz + 1 < h.oz + h.hz && w.cx >= 1 && w.cy >= 1 && w.cz >= 1 &&
+           w.cx + 1 < (int32_t)sd.X && w.cy + 1 < (int32_t)sd.Y && w.cz + 1 < (int32_t)sd.Z;
+}
+
+// Scene-local cell of halo index i, or false when it lies outside the grid.
+__device__ __forceinline__ bool halo_cell(const ChunkHdr& h, const SceneDesc& sd, int i, uint32_t& cell) {
+    const int hxy = h.hx * h.hy;
+    const int32_t x = h.ox + i % h.hx, y = h.oy + (i / h.hx) % h.hy, z = h.oz + i / hxy;
+    if (x < 0 || y < 0 || z < 0 || x >= (int32_t)sd.X || y >= (int32_t)sd.Y || z >= (int32_t)sd.Z) return false;
+    cell = local_cell(sd, x, y, z);
+    return true;
+}
+
+// Add into a shared accumulator (wrapping i32, as the reference's atomics).
+// Aggregated: lanes of `grp` (same stencil base) sum their values with one
+// warp reduction and one lane adds the sum.
+__device__ __forceinline__ void agg_add(int32_t* slot, int32_t val, uint32_t grp, bool leader) {
+#if MPM_P2G_AGG
+    const int32_t s = __reduce_add_sync(grp, val);
+    if (leader) atomicAdd(slot, s);
+#else
+    (void)grp;
+    (void)leader;
+    atomicAdd(slot, val);
+#endif
+}
+
+// Lanes sharing a stencil base (aggregated mode only).
+__device__ __forceinline__ uint32_t agg_group(bool shared_path, int hb, uint32_t lane, bool& leader) {
+#if MPM_P2G_AGG
+    const uint32_t grp = __match_any_sync(0xffffffffu, shared_path ? (uint32_t)hb : 0x80000000u + lane);
+    leader = (uint32_t)(__ffs(grp) - 1) == lane;
+    return grp;
+#else
+    (void)shared_path;
+    (void)hb;
+    leader = true;
+    return 1u << lane;
+#endif
+}
+
+// ---------------------------------------------------------------------------
+// P2G_MASS (shaders.js:242-274): one block per chunk, one thread per particle
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, const float4* __restrict__ posm,
+                                                                   int32_t* __restrict__ cm) {
+    constexpr int kPer = kChunk / kChunkThreads;
+    __shared__ int32_t acc[kHaloCells];
+    const uint32_t nch = v.ctrl->total_chunks;
+    const uint32_t lane = threadIdx.x & 31;
+    __shared__ ChunkHdr hs;
+    for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+        if (threadIdx.x == 0) chunk_header(v, ch, hs);
+        __syncthreads();
+        const ChunkHdr h = hs;
+        // this thread's particles, in flight while the halo is cleared
+        float4 q[kPer];
 #pragma unroll
-        for (int q = 0; q < 27; ++q) acc[q] = 0;
-        uint32_t slot_n = it.b > 1 ? v.perm[it.pbase + 32u] : 0u;
-        float4 p_c = posm[v.perm[it.pbase]];
-        for (uint32_t k = 0; k < it.b; ++k) {
-            float4 p_n = p_c;
-            uint32_t slot_nn = slot_n;
-            if (k + 1 < it.b) {
-                p_n = posm[slot_n];
-                if (k + 2 < it.b) slot_nn = v.perm[it.pbase + (k + 2) * 32u];
-            }
-            const float4 p = p_c;
-            p_c = p_n;
-            slot_n = slot_nn;
-            const PW w = particle_weights(p.x, p.y, p.z);
-            // weight <= 0.4219: for |mass| < 47000 encode's clamp is the identity
-            const bool safe = fabsf(p.w) < 47000.0f;
-            if (w.cx == ix && w.cy == iy && w.cz == iz) {
-                float wxy[9];
+        for (int r = 0; r < kPer; ++r) {
+            const uint32_t p = h.first + r * kChunkThreads + chunk_lane_offset();
+            q[r] = p < h.end ? posm[v.perm[p]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        const int hn = h.hx * h.hy * h.hz, hxy = h.hx * h.hy;
+        for (int i = threadIdx.x; i < hn; i += blockDim.x) acc[i] = 0;
+        __syncthreads();
+        const SceneDesc& sd = v.scenes[h.scene];
 #pragma unroll
-                for (int j = 0; j < 3; ++j)
+        for (int r = 0; r < kPer; ++r) {
+            const bool valid = h.first + r * kChunkThreads + chunk_lane_offset() < h.end;
+            const PW w = particle_weights(q[r].x, q[r].y, q[r].z);
+            const bool fast = valid && in_halo(w, h, sd);
+            const int hb = ((w.cz - 1 - h.oz) * h.hy + (w.cy - 1 - h.oy)) * h.hx + (w.cx - 1 - h.ox);
+            bool leader;
+            const uint32_t grp = agg_group(fast, hb, lane, leader);
+            if (fast) {
+                // weight <= 0.4219: for |mass| < 47000 encode's clamp is the identity
+                const bool safe = fabsf(q[r].w) < 47000.0f;
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) wxy[j * 3 + i] = w.wx[i] * w.wy[j];
-                if (safe) {
+                for (int kk = 0; kk < 3; ++kk)
 #pragma unroll
-                    for (int kk = 0; kk < 3; ++kk)
+                    for (int j = 0; j < 3; ++j)
 #pragma unroll
-                        for (int q = 0; q < 9; ++q) acc[kk * 9 + q] += encode_unclamped(wxy[q] * w.wz[kk] * p.w);
-                } else {
-#pragma unroll
-                    for (int kk = 0; kk < 3; ++kk)
-#pragma unroll
-                        for (int q = 0; q < 9; ++q) acc[kk * 9 + q] += encode(wxy[q] * w.wz[kk] * p.w);
-                }
-            } else {
-                // particle outside its item's cell (positions outside the grid): per-particle path
+                        for (int i = 0; i < 3; ++i) {
+                            const float x = w.wx[i] * w.wy[j] * w.wz[kk] * q[r].w;
+                            const int32_t e = safe ? encode_unclamped(x) : encode(x);
+                            agg_add(&acc[hb + kk * hxy + j * h.hx + i], e, grp, leader);
+                        }
+            } else if (valid) {
+                // stencil outside the halo or the grid: bounds-checked global atomics
+                const int32_t X = sd.X, Y = sd.Y, Z = sd.Z;
+                int32_t* scm = cm + sd.cell_base;
                 for (int kk = 0; kk < 3; ++kk)
                     for (int j = 0; j < 3; ++j)
                         for (int i = 0; i < 3; ++i) {
                             const int32_t xx = w.cx - 1 + i, yy = w.cy - 1 + j, zz = w.cz - 1 + kk;
                             if (xx < 0 || xx >= X || yy < 0 || yy >= Y || zz < 0 || zz >= Z) continue;
                             const float ww = w.wx[i] * w.wy[j] * w.wz[kk];
-                            atomicAdd(&scm[(zz * Y + yy) * X + xx], encode(ww * p.w));
+                            atomicAdd(&scm[(zz * Y + yy) * X + xx], encode(ww * q[r].w));
                         }
             }
         }
-#pragma unroll
-        for (int kk = 0; kk < 3; ++kk)
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const int32_t xx = ix - 1 + i, yy = iy - 1 + j, zz = iz - 1 + kk;
-                    const int32_t a = acc[kk * 9 + j * 3 + i];
-                    if (a != 0 && xx >= 0 && xx < X && yy >= 0 && yy < Y && zz >= 0 && zz < Z)
-                        atomicAdd(&scm[(zz * Y + yy) * X + xx], a);
-                }
+        __syncthreads();
+        int32_t* scm = cm + sd.cell_base;
+        for (int i = threadIdx.x; i < hn; i += blockDim.x) {
+            const int32_t a = acc[i];
+            uint32_t cell;
+            if (a != 0 && halo_cell(h, sd, i, cell)) atomicAdd(&scm[cell], a);
+        }
+        __syncthreads();
     }
 }
 
@@ -728,213 +756,261 @@ __global__ void __launch_bounds__(256) k_update_tiles(WorldView v, const int32_t
     }
 }
 
+
 // ---------------------------------------------------------------------------
-// P2G_MOM (shaders.js:276-371), item-major
+// P2G_MOM (shaders.js:276-371): one block per chunk, one thread per particle
 // ---------------------------------------------------------------------------
 struct MomIn {
     float vx, vy, vz, m;
     float a00, a01, a02, a10, a11, a12, a20, a21, a22;
 };
 
-// Per-thread accumulator slots of k_p2g_mom_items (81 x 4 B per thread).
-__shared__ int32_t g_sacc[81][kItemThreads];
-
-// The scatter part of P2G_MOM for one particle whose density is known.
-// kDirect: atomics straight into the grid at the particle's own stencil;
-// otherwise the 81 encoded contributions are added into the shared slots.
-// kClamp: full encode; without it the caller has bounded every value inside
-// +-20000, where encode's clamp is the identity.
-template <bool kDirect, bool kClamp>
-__device__ __forceinline__ void mom_scatter(const PW& w, const MomIn& in, const float* s, float coef, uint32_t X,
-                                            uint32_t SLICE, int32_t* mv, uint32_t baseIdx, uint32_t G) {
+// The 81 encoded momentum contributions of one particle (shaders.js:340-370),
+// handed to sink(k, j, i, ex, ey, ez).  Every value is the reference's own
+// expression, (C d) = (c0 dx + c1 dy) + c2 dz and (S d) likewise, with the
+// products along the third axis and the (dx, dy) partial sums computed once
+// and reused (the same roundings, fewer instructions).  kClamp: full encode;
+// without it the caller has bounded every value inside +-20000, where the
+// clamp is the identity.
+template <bool kClamp, class Sink>
+__device__ __forceinline__ void mom_contrib(const PW& w, const MomIn& in, const float* s, float coef, Sink&& sink) {
     const float s00 = s[0], s11 = s[1], s22 = s[2], s01 = s[3], s02 = s[4], s12 = s[5];
     const float dxs[3] = {-w.fx - 1.0f, -w.fx, 1.0f - w.fx};
     const float dys[3] = {-w.fy - 1.0f, -w.fy, 1.0f - w.fy};
     const float dzs[3] = {-w.fz - 1.0f, -w.fz, 1.0f - w.fz};
-#pragma unroll 1
+    float qz[3][3], fz[3][3];   // [component][k]: C[c][2] dz_k and S[c][2] dz_k
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const float wzk = k == 0 ? w.wz[0] : (k == 1 ? w.wz[1] : w.wz[2]);
-        const float dzk = k == 0 ? dzs[0] : (k == 1 ? dzs[1] : dzs[2]);
+        qz[0][k] = in.a02 * dzs[k];
+        qz[1][k] = in.a12 * dzs[k];
+        qz[2][k] = in.a22 * dzs[k];
+        fz[0][k] = s02 * dzs[k];
+        fz[1][k] = s12 * dzs[k];
+        fz[2][k] = s22 * dzs[k];
+    }
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const float wyzk = w.wy[j] * wzk, dyj = dys[j];
+    for (int j = 0; j < 3; ++j) {
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const float ww = w.wx[i] * wyzk;
-                const float dxi = dxs[i];
-                const float Qx = in.a00 * dxi + in.a01 * dyj + in.a02 * dzk;
-                const float Qy = in.a10 * dxi + in.a11 * dyj + in.a12 * dzk;
-                const float Qz = in.a20 * dxi + in.a21 * dyj + in.a22 * dzk;
-                const float fxf = coef * (s00 * dxi + s01 * dyj + s02 * dzk);
-                const float fyf = coef * (s01 * dxi + s11 * dyj + s12 * dzk);
-                const float fzf = coef * (s02 * dxi + s12 * dyj + s22 * dzk);
+        for (int i = 0; i < 3; ++i) {
+            const float dxi = dxs[i], dyj = dys[j];
+            const float qx = in.a00 * dxi + in.a01 * dyj;
+            const float qy = in.a10 * dxi + in.a11 * dyj;
+            const float qzz = in.a20 * dxi + in.a21 * dyj;
+            const float gx = s00 * dxi + s01 * dyj;
+            const float gy = s01 * dxi + s11 * dyj;
+            const float gz = s02 * dxi + s12 * dyj;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float ww = w.wx[i] * (w.wy[j] * w.wz[k]);
+                const float Qx = qx + qz[0][k];
+                const float Qy = qy + qz[1][k];
+                const float Qz = qzz + qz[2][k];
+                const float fxf = coef * (gx + fz[0][k]);
+                const float fyf = coef * (gy + fz[1][k]);
+                const float fzf = coef * (gz + fz[2][k]);
                 const float vx = ww * (in.m * (in.vx + Qx) + fxf);
                 const float vy = ww * (in.m * (in.vy + Qy) + fyf);
                 const float vz = ww * (in.m * (in.vz + Qz) + fzf);
-                const int32_t ex = kClamp ? encode(vx) : encode_unclamped(vx);
-                const int32_t ey = kClamp ? encode(vy) : encode_unclamped(vy);
-                const int32_t ez = kClamp ? encode(vz) : encode_unclamped(vz);
-                if (kDirect) {
-                    const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
-                    if (cidx < G) {
-                        atomicAdd(mv + 3ull * cidx + 0, ex);
-                        atomicAdd(mv + 3ull * cidx + 1, ey);
-                        atomicAdd(mv + 3ull * cidx + 2, ez);
-                    }
-                } else {
-                    const int q = (k * 9 + j * 3 + i) * 3;
-                    atomicAdd(&g_sacc[q + 0][threadIdx.x], ex);
-                    atomicAdd(&g_sacc[q + 1][threadIdx.x], ey);
-                    atomicAdd(&g_sacc[q + 2][threadIdx.x], ez);
-                }
+                sink(k, j, i, kClamp ? encode(vx) : encode_unclamped(vx), kClamp ? encode(vy) : encode_unclamped(vy),
+                     kClamp ? encode(vz) : encode_unclamped(vz));
             }
         }
     }
 }
 
-__global__ void __launch_bounds__(kItemThreads, MPM_MOM_LB) k_p2g_mom_items(WorldView v,
-                                                                             const float4* __restrict__ posm,
-                                                                             const float4* __restrict__ velid,
-                                                                             const float* __restrict__ aff,
-                                                                             const float* __restrict__ cmf,
-                                                                             int32_t* __restrict__ mv,
-                                                                             float* __restrict__ dens) {
-    __shared__ ItemTables tabs;
-    load_tables(v, tabs);
-    const uint32_t nitems = v.ctrl->total_items;
-    const size_t plane = v.npos;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nitems; g += gridDim.x * blockDim.x) {
-        const ItemRef it = item_ref(v, tabs, g);
-        if (!it.valid) continue;
-        const SceneDesc& sd = v.scenes[it.scene];
-        const uint32_t X = sd.X, SLICE = sd.X * sd.Y, G = sd.G;
-        const float* scmf = cmf + sd.cell_base;
-        int32_t* smv = mv + 3ull * sd.cell_base;
-        int32_t ix, iy, iz;
-        cell_xyz(sd, it.cell, ix, iy, iz);
-        const uint32_t ibase = (uint32_t)(((iz - 1) * (int32_t)sd.Y + (iy - 1)) * (int32_t)X + (ix - 1));
-        float m27[27];
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const uint32_t cidx = ibase + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
-                    m27[k * 9 + j * 3 + i] = cidx < G ? scmf[cidx] : 0.0f;
-                }
-#pragma unroll
-        for (int q = 0; q < 81; ++q) g_sacc[q][threadIdx.x] = 0;
-        const float rest = sd.P.rest_density, stiff = sd.P.stiffness, eos = sd.P.eos_power, visc = sd.P.viscosity;
-        const float dt = sd.P.dt;
-        // software pipeline: the next particle's permutation entry and record are
-        // loaded while the current one is processed
-        uint32_t slot_n = it.b > 1 ? v.perm[it.pbase + 32u] : 0u;
-        float4 p_c, v_c;
-        float a_c[9];
-        {
-            const uint32_t slot = v.perm[it.pbase];
-            p_c = posm[slot];
-            v_c = velid[slot];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) a_c[e] = aff[e * plane + slot];
-        }
-        for (uint32_t kk = 0; kk < it.b; ++kk) {
-            const uint32_t pos = it.pbase + kk * 32u;
-            float4 p_n = p_c, v_n = v_c;
-            float a_n[9];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) a_n[e] = a_c[e];
-            uint32_t slot_nn = slot_n;
-            if (kk + 1 < it.b) {
-                p_n = posm[slot_n];
-                v_n = velid[slot_n];
-#pragma unroll
-                for (int e = 0; e < 9; ++e) a_n[e] = aff[e * plane + slot_n];
-                if (kk + 2 < it.b) slot_nn = v.perm[pos + 64u];
-            }
-            const float4 p = p_c;
-            const MomIn in{v_c.x, v_c.y, v_c.z, p.w, a_c[0], a_c[1], a_c[2], a_c[3], a_c[4], a_c[5],
-                           a_c[6], a_c[7], a_c[8]};
-            p_c = p_n;
-            v_c = v_n;
-#pragma unroll
-            for (int e = 0; e < 9; ++e) a_c[e] = a_n[e];
-            slot_n = slot_nn;
-            const PW w = particle_weights(p.x, p.y, p.z);
-            const bool same = (w.cx == ix && w.cy == iy && w.cz == iz);
-            const uint32_t baseIdx = (uint32_t)(((w.cz - 1) * (int32_t)sd.Y + (w.cy - 1)) * (int32_t)X + (w.cx - 1));
-            float density = 0.0f;
-            if (same) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-#pragma unroll
-                    for (int jj = 0; jj < 3; ++jj)
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) density += w.wx[i] * w.wy[jj] * w.wz[k] * m27[k * 9 + jj * 3 + i];
-            } else {
-                for (int k = 0; k < 3; ++k)
-                    for (int jj = 0; jj < 3; ++jj)
-                        for (int i = 0; i < 3; ++i) {
-                            const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)jj * X + (uint32_t)i;
-                            const float cmass = cidx < G ? scmf[cidx] : 0.0f;
-                            density += w.wx[i] * w.wy[jj] * w.wz[k] * cmass;
-                        }
-            }
-            dens[pos] = density;
-            if (density <= 1e-8f) continue;
-            // stress (shaders.js:325-338)
-            const float vol = __fdiv_rn(in.m, fmaxf(density, rest * 0.15f));
-            float pressure = stiff * (eos_pow(__fdiv_rn(density, rest), eos) - 1.0f);
-            const float pFloor = density > rest * kCohesionGate ? kCohesionPressure : 0.0f;
-            pressure = fmaxf(pressure, pFloor);
-            float s[6];
-            s[0] = -pressure + visc * (in.a00 + in.a00);
-            s[1] = -pressure + visc * (in.a11 + in.a11);
-            s[2] = -pressure + visc * (in.a22 + in.a22);
-            s[3] = visc * (in.a01 + in.a10);
-            s[4] = visc * (in.a02 + in.a20);
-            s[5] = visc * (in.a12 + in.a21);
-            const float coef = -vol * 4.0f * dt;
-            // |value| <= 0.4219 * (|m| (|v| + 1.5 |A row|_1) + |coef| 1.5 |S row|_1): when that bound
-            // is well inside +-20000 encode's clamp cannot change any value (NaN/Inf fail the test).
-            const float am = fabsf(in.m), ac = fabsf(coef);
-            const float bx = am * (fabsf(in.vx) + 1.5f * (fabsf(in.a00) + fabsf(in.a01) + fabsf(in.a02))) +
-                             ac * 1.5f * (fabsf(s[0]) + fabsf(s[3]) + fabsf(s[4]));
-            const float by = am * (fabsf(in.vy) + 1.5f * (fabsf(in.a10) + fabsf(in.a11) + fabsf(in.a12))) +
-                             ac * 1.5f * (fabsf(s[3]) + fabsf(s[1]) + fabsf(s[5]));
-            const float bz = am * (fabsf(in.vz) + 1.5f * (fabsf(in.a20) + fabsf(in.a21) + fabsf(in.a22))) +
-                             ac * 1.5f * (fabsf(s[4]) + fabsf(s[5]) + fabsf(s[2]));
-            const bool safe = fmaxf(bx, fmaxf(by, bz)) * 0.4222f < 19000.0f;
-            if (same) {
-                if (safe) mom_scatter<false, false>(w, in, s, coef, X, SLICE, smv, baseIdx, G);
-                else mom_scatter<false, true>(w, in, s, coef, X, SLICE, smv, baseIdx, G);
-            } else {
-                mom_scatter<true, true>(w, in, s, coef, X, SLICE, smv, baseIdx, G);
-            }
-        }
+// P2G_MOM for one particle whose inputs are loaded.
+__device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr& h, const SceneDesc& sd, bool valid,
+                                             uint32_t p, const float4 pm, const float4 vi, const float* a,
+                                             const float* mh, int32_t (*acc)[kHaloCells],
+                                             const float* __restrict__ scmf, int32_t* __restrict__ smv,
+                                             float* __restrict__ dens, uint32_t lane) {
+    const int hxy = h.hx * h.hy;
+    const uint32_t X = sd.X, SLICE = sd.X * sd.Y, G = sd.G;
+    const PW w = particle_weights(pm.x, pm.y, pm.z);
+    const bool fast = valid && in_halo(w, h, sd);
+    const int hb = ((w.cz - 1 - h.oz) * h.hy + (w.cy - 1 - h.oy)) * h.hx + (w.cx - 1 - h.ox);
+    const uint32_t baseIdx = (uint32_t)(((w.cz - 1) * (int32_t)sd.Y + (w.cy - 1)) * (int32_t)X + (w.cx - 1));
+    // density (shaders.js:305-313), k, j, i order
+    float density = 0.0f;
+    if (fast) {
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int jj = 0; jj < 3; ++jj)
 #pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    density += w.wx[i] * w.wy[jj] * w.wz[k] * mh[hb + k * hxy + jj * h.hx + i];
+    } else if (valid) {
+        for (int k = 0; k < 3; ++k)
+            for (int jj = 0; jj < 3; ++jj)
                 for (int i = 0; i < 3; ++i) {
-                    const uint32_t cidx = ibase + (uint32_t)k * SLICE + (uint32_t)jj * X + (uint32_t)i;
-                    const int q = (k * 9 + jj * 3 + i) * 3;
-                    const int32_t a0 = g_sacc[q + 0][threadIdx.x], a1 = g_sacc[q + 1][threadIdx.x],
-                                  a2 = g_sacc[q + 2][threadIdx.x];
-                    if (cidx < G) {
-                        if (a0) atomicAdd(smv + 3ull * cidx + 0, a0);
-                        if (a1) atomicAdd(smv + 3ull * cidx + 1, a1);
-                        if (a2) atomicAdd(smv + 3ull * cidx + 2, a2);
-                    }
+                    const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)jj * X + (uint32_t)i;
+                    const float cmass = cidx < G ? scmf[cidx] : 0.0f;
+                    density += w.wx[i] * w.wy[jj] * w.wz[k] * cmass;
                 }
+    }
+    if (valid) dens[p] = density;
+    const bool live = valid && density > 1e-8f;   // shaders.js:315
+    // stress (shaders.js:325-338)
+    const float rest = sd.P.rest_density;
+    const MomIn in{vi.x, vi.y, vi.z, pm.w, a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]};
+    const float vol = __fdiv_rn(in.m, fmaxf(density, rest * 0.15f));
+    float pressure = sd.P.stiffness * (eos_pow(__fdiv_rn(density, rest), sd.P.eos_power) - 1.0f);
+    const float pFloor = density > rest * kCohesionGate ? kCohesionPressure : 0.0f;
+    pressure = fmaxf(pressure, pFloor);
+    const float visc = sd.P.viscosity;
+    float s[6];
+    s[0] = -pressure + visc * (in.a00 + in.a00);
+    s[1] = -pressure + visc * (in.a11 + in.a11);
+    s[2] = -pressure + visc * (in.a22 + in.a22);
+    s[3] = visc * (in.a01 + in.a10);
+    s[4] = visc * (in.a02 + in.a20);
+    s[5] = visc * (in.a12 + in.a21);
+    const float coef = -vol * 4.0f * sd.P.dt;
+    // |value| <= 0.4219 * (|m| (|v| + 1.5 |A row|_1) + |coef| 1.5 |S row|_1): when that bound
+    // is well inside +-20000 encode's clamp cannot change any value (NaN/Inf fail the test).
+    const float am = fabsf(in.m), ac = fabsf(coef);
+    const float bx = am * (fabsf(in.vx) + 1.5f * (fabsf(in.a00) + fabsf(in.a01) + fabsf(in.a02))) +
+                     ac * 1.5f * (fabsf(s[0]) + fabsf(s[3]) + fabsf(s[4]));
+    const float by = am * (fabsf(in.vy) + 1.5f * (fabsf(in.a10) + fabsf(in.a11) + fabsf(in.a12))) +
+                     ac * 1.5f * (fabsf(s[3]) + fabsf(s[1]) + fabsf(s[5]));
+    const float bz = am * (fabsf(in.vz) + 1.5f * (fabsf(in.a20) + fabsf(in.a21) + fabsf(in.a22))) +
+                     ac * 1.5f * (fabsf(s[4]) + fabsf(s[5]) + fabsf(s[2]));
+    const bool safe = fmaxf(bx, fmaxf(by, bz)) * 0.4222f < 19000.0f;
+    const bool shared_path = live && fast;
+    bool leader;
+    const uint32_t grp = agg_group(shared_path, hb, lane, leader);
+    if (shared_path) {
+        auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
+            const int hi = hb + k * hxy + j * h.hx + i;
+            agg_add(&acc[0][hi], ex, grp, leader);
+            agg_add(&acc[1][hi], ey, grp, leader);
+            agg_add(&acc[2][hi], ez, grp, leader);
+        };
+        // the clamp-free form only when the whole group can use it
+        if (__all_sync(grp, safe)) mom_contrib<false>(w, in, s, coef, sink);
+        else mom_contrib<true>(w, in, s, coef, sink);
+    } else if (live) {
+        auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
+            const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
+            if (cidx < G) {
+                atomicAdd(smv + 3ull * cidx + 0, ex);
+                atomicAdd(smv + 3ull * cidx + 1, ey);
+                atomicAdd(smv + 3ull * cidx + 2, ez);
+            }
+        };
+        mom_contrib<true>(w, in, s, coef, sink);
+    }
+}
+
+#ifndef MPM_MOM_PREFETCH
+#define MPM_MOM_PREFETCH 1
+#endif
+#ifndef MPM_MOM_MINB
+#define MPM_MOM_MINB 2
+#endif
+#ifndef MPM_G2P_PREFETCH
+#define MPM_G2P_PREFETCH 0
+#endif
+
+__global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(WorldView v, const float4* __restrict__ posm,
+                                                                     const float4* __restrict__ velid,
+                                                                     const float* __restrict__ aff,
+                                                                     const float* __restrict__ cmf,
+                                                                     int32_t* __restrict__ mv,
+                                                                     float* __restrict__ dens) {
+    constexpr int kPer = kChunk / kChunkThreads;
+    __shared__ float mh[kHaloCells];
+    __shared__ int32_t acc[3][kHaloCells];
+    const uint32_t nch = v.ctrl->total_chunks;
+    const uint32_t lane = threadIdx.x & 31;
+    const size_t plane = v.npos;
+    __shared__ ChunkHdr hs;
+    for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+        if (threadIdx.x == 0) chunk_header(v, ch, hs);
+        __syncthreads();
+        const ChunkHdr h = hs;
+        const SceneDesc& sd = v.scenes[h.scene];
+        const float* scmf = cmf + sd.cell_base;
+        int32_t* smv = mv + 3ull * sd.cell_base;
+        // the first particle's inputs are in flight while the halo is staged
+        uint32_t p = h.first + chunk_lane_offset();
+        bool valid = p < h.end;
+        float4 pm = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vi = pm;
+        float a[9];
+        {
+            const uint32_t slot = valid ? v.perm[p] : 0u;
+            if (valid) {
+                pm = posm[slot];
+                vi = velid[slot];
+            }
+#pragma unroll
+            for (int e = 0; e < 9; ++e) a[e] = valid ? aff[e * plane + slot] : 0.0f;
+        }
+        const int hn = h.hx * h.hy * h.hz;
+        for (int i = threadIdx.x; i < hn; i += blockDim.x) {
+            uint32_t cell;
+            mh[i] = halo_cell(h, sd, i, cell) ? scmf[cell] : 0.0f;
+            acc[0][i] = 0;
+            acc[1][i] = 0;
+            acc[2][i] = 0;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int r = 0; r < kPer; ++r) {
+            // next particle's inputs
+            const uint32_t pn = p + kChunkThreads;
+            const bool vn = r + 1 < kPer && pn < h.end;
+            float4 pmn = pm, vin = vi;
+            float an[9];
+#if MPM_MOM_PREFETCH
+            {
+                const uint32_t slot = vn ? v.perm[pn] : 0u;
+                if (vn) {
+                    pmn = posm[slot];
+                    vin = velid[slot];
+                }
+#pragma unroll
+                for (int e = 0; e < 9; ++e) an[e] = vn ? aff[e * plane + slot] : 0.0f;
+            }
+#endif
+            mom_particle(v, h, sd, valid, p, pm, vi, a, mh, acc, scmf, smv, dens, lane);
+#if !MPM_MOM_PREFETCH
+            {
+                const uint32_t slot = vn ? v.perm[pn] : 0u;
+                if (vn) {
+                    pmn = posm[slot];
+                    vin = velid[slot];
+                }
+#pragma unroll
+                for (int e = 0; e < 9; ++e) an[e] = vn ? aff[e * plane + slot] : 0.0f;
+            }
+#endif
+            p = pn;
+            valid = vn;
+            pm = pmn;
+            vi = vin;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) a[e] = an[e];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < hn; i += blockDim.x) {
+            const int32_t a0 = acc[0][i], a1 = acc[1][i], a2 = acc[2][i];
+            uint32_t cell;
+            if ((a0 | a1 | a2) != 0 && halo_cell(h, sd, i, cell)) {
+                int32_t* d = smv + 3ull * cell;
+                if (a0) atomicAdd(d + 0, a0);
+                if (a1) atomicAdd(d + 1, a1);
+                if (a2) atomicAdd(d + 2, a2);
+            }
+        }
+        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
-// G2P (shaders.js:579-705), item-major, + binning of the new positions and
-// the diffuse spawn decision (shaders.js:800-855).
+// G2P (shaders.js:579-705): one block per chunk, one thread per particle,
+// + binning of the new positions and the diffuse spawn decision (shaders.js:800-855).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool estimate_normal_f(const float* __restrict__ cmf, const SceneDesc& sd, float px,
                                                   float py, float pz, f3& n) {
@@ -1044,8 +1120,8 @@ __device__ __forceinline__ void g2p_finish(const float4 q, float gvx, float gvy,
     if (np.z > P.hard_max_z) { np.z = P.hard_max_z; nv.z = 0.0f; }
 }
 
-// G2P gather for a particle outside its item's cell (positions outside the
-// grid): the reference's linear stencil index with a bounds guard.
+// G2P gather for a particle whose stencil leaves the halo box or the grid:
+// the reference's linear stencil index with a bounds guard.
 __device__ __noinline__ void g2p_gather_direct(const PW& w, const float4 q, const float* __restrict__ mvf, uint32_t X,
                                                uint32_t Y, uint32_t G, float& gvx, float& gvy, float& gvz,
                                                float* B) {
@@ -1077,83 +1153,77 @@ __device__ __noinline__ void g2p_gather_direct(const PW& w, const float4 q, cons
     }
 }
 
-__global__ void __launch_bounds__(kItemThreads, MPM_G2P_LB) k_g2p_items(WorldView v,
-                                                                         const float4* __restrict__ posm,
-                                                                         const float4* __restrict__ velid,
-                                                                         const float* __restrict__ mvf,
-                                                                         const float* __restrict__ cmf,
-                                                                         float4* __restrict__ posm_out,
-                                                                         float4* __restrict__ velid_out,
-                                                                         float* __restrict__ aff_out, DiffuseView dv) {
-    __shared__ ItemTables tabs;
-    load_tables(v, tabs);
-    const uint32_t nitems = v.ctrl->total_items;
+
+__global__ void __launch_bounds__(kChunkThreads) k_g2p_chunks(WorldView v, const float4* __restrict__ posm,
+                                                              const float4* __restrict__ velid,
+                                                              const float* __restrict__ mvf,
+                                                              const float* __restrict__ cmf,
+                                                              float4* __restrict__ posm_out,
+                                                              float4* __restrict__ velid_out,
+                                                              float* __restrict__ aff_out, DiffuseView dv) {
+    constexpr int kPer = kChunk / kChunkThreads;
+    __shared__ float vh[3][kHaloCells];
+    const uint32_t nch = v.ctrl->total_chunks;
     const size_t plane = v.npos;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nitems; g += gridDim.x * blockDim.x) {
-        const ItemRef it = item_ref(v, tabs, g);
-        if (!it.valid) {
-            // padding lane: mark its positions as holes for the next binning and the export
-            for (uint32_t kk = 0; kk < it.b; ++kk) {
-                const uint32_t pos = it.pbase + kk * 32u;
-                if (pos < v.npos) {
-                    v.key[pos] = kHole;
-                    velid_out[pos] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(kHole));
-                }
+    __shared__ ChunkHdr hs;
+    for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+        // one thread reads the chunk header (measured faster here than every thread reading it)
+        if (threadIdx.x == 0) chunk_header(v, ch, hs);
+        __syncthreads();
+        const ChunkHdr h = hs;
+        const SceneDesc& sd = v.scenes[h.scene];
+#if MPM_G2P_PREFETCH
+        // this thread's particles, in flight while the halo is staged
+        float4 qs[kPer], vis[kPer];
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) {
+            const uint32_t p = h.first + r * kChunkThreads + threadIdx.x;
+            if (p < h.end) {
+                const uint32_t slot = v.perm[p];
+                qs[r] = posm[slot];
+                vis[r] = velid[slot];
+            } else {
+                qs[r] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                vis[r] = qs[r];
             }
-            continue;
         }
-        const SceneDesc& sd = v.scenes[it.scene];
-        const uint32_t X = sd.X, SLICE = sd.X * sd.Y, G = sd.G;
+#endif
+        const int hn = h.hx * h.hy * h.hz, hxy = h.hx * h.hy;
         const float* smvf = mvf + 3ull * sd.cell_base;
-        int32_t ix, iy, iz;
-        cell_xyz(sd, it.cell, ix, iy, iz);
-        const uint32_t item_tile = tile_of(sd, ix, iy, iz);
-        mark_occupied(v, item_tile);
-        const uint32_t ibase = (uint32_t)(((iz - 1) * (int32_t)sd.Y + (iy - 1)) * (int32_t)X + (ix - 1));
-        float cv[81];
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const uint32_t cidx = ibase + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
-                    const int q = (k * 9 + j * 3 + i) * 3;
-                    if (cidx < G) {
-                        const float* c = smvf + 3ull * cidx;
-                        cv[q + 0] = c[0]; cv[q + 1] = c[1]; cv[q + 2] = c[2];
-                    } else {
-                        cv[q + 0] = 0.0f; cv[q + 1] = 0.0f; cv[q + 2] = 0.0f;
-                    }
-                }
-        const bool spawn_scene = dv.enabled && it.scene == dv.scene;
-        uint32_t slot_n = it.b > 1 ? v.perm[it.pbase + 32u] : 0u;
-        float4 q_c, vi_c;
-        {
-            const uint32_t slot = v.perm[it.pbase];
-            q_c = posm[slot];
-            vi_c = velid[slot];
-        }
-        for (uint32_t kk = 0; kk < it.b; ++kk) {
-            const uint32_t pos = it.pbase + kk * 32u;
-            float4 q_n = q_c, vi_n = vi_c;
-            uint32_t slot_nn = slot_n;
-            if (kk + 1 < it.b) {
-                q_n = posm[slot_n];
-                vi_n = velid[slot_n];
-                if (kk + 2 < it.b) slot_nn = v.perm[pos + 64u];
+        for (int i = threadIdx.x; i < hn; i += blockDim.x) {
+            uint32_t cell;
+            if (halo_cell(h, sd, i, cell)) {
+                const float* c = smvf + 3ull * cell;
+                vh[0][i] = c[0];
+                vh[1][i] = c[1];
+                vh[2][i] = c[2];
+            } else {
+                vh[0][i] = 0.0f;
+                vh[1][i] = 0.0f;
+                vh[2][i] = 0.0f;
             }
-            const float4 q = q_c;
-            const float4 vi = vi_c;
-            q_c = q_n;
-            vi_c = vi_n;
-            slot_n = slot_nn;
+        }
+        __syncthreads();
+        const bool spawn_scene = dv.enabled && h.scene == dv.scene;
+        const uint32_t X = sd.X, G = sd.G;
+#pragma unroll 1
+        for (int r = 0; r < kPer; ++r) {
+            const uint32_t p = h.first + r * kChunkThreads + threadIdx.x;
+            if (p >= h.end) break;
+#if MPM_G2P_PREFETCH
+            const float4 q = qs[r];
+            const float4 vi = vis[r];
+#else
+            const uint32_t slot = v.perm[p];
+            const float4 q = posm[slot];
+            const float4 vi = velid[slot];
+#endif
             const PW w = particle_weights(q.x, q.y, q.z);
-            const bool same = (w.cx == ix && w.cy == iy && w.cz == iz);
             float gvx = 0.0f, gvy = 0.0f, gvz = 0.0f;
             float B[9] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-            if (same) {
+            if (in_halo(w, h, sd)) {
                 const int32_t bx = w.cx - 1, by = w.cy - 1, bz = w.cz - 1;
+                const int hb = ((bz - h.oz) * h.hy + (by - h.oy)) * h.hx + (bx - h.ox);
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     const float wzk = w.wz[k];
@@ -1166,8 +1236,8 @@ __global__ void __launch_bounds__(kItemThreads, MPM_G2P_LB) k_g2p_items(WorldVie
                         for (int i = 0; i < 3; ++i) {
                             const float ww = w.wx[i] * wyzk;
                             const float dxi = __int2float_rn(bx + i) - q.x + 0.5f;
-                            const int qq = (k * 9 + jj * 3 + i) * 3;
-                            const float wvx = ww * cv[qq + 0], wvy = ww * cv[qq + 1], wvz = ww * cv[qq + 2];
+                            const int hi = hb + k * hxy + jj * h.hx + i;
+                            const float wvx = ww * vh[0][hi], wvy = ww * vh[1][hi], wvz = ww * vh[2][hi];
                             gvx += wvx; gvy += wvy; gvz += wvz;
                             B[0] += wvx * dxi; B[1] += wvx * dyj; B[2] += wvx * dzk;
                             B[3] += wvy * dxi; B[4] += wvy * dyj; B[5] += wvy * dzk;
@@ -1179,28 +1249,25 @@ __global__ void __launch_bounds__(kItemThreads, MPM_G2P_LB) k_g2p_items(WorldVie
                 g2p_gather_direct(w, q, smvf, X, sd.Y, G, gvx, gvy, gvz, B);
             }
 #pragma unroll
-            for (int e = 0; e < 9; ++e) aff_out[e * plane + pos] = B[e] * 4.0f;
+            for (int e = 0; e < 9; ++e) aff_out[e * plane + p] = B[e] * 4.0f;
             f3 np, nv;
             g2p_finish(q, gvx, gvy, gvz, sd.P, sd.W, np, nv);
-            posm_out[pos] = make_float4(np.x, np.y, np.z, q.w);
-            velid_out[pos] = make_float4(nv.x, nv.y, nv.z, vi.w);
+            posm_out[p] = make_float4(np.x, np.y, np.z, q.w);
+            velid_out[p] = make_float4(nv.x, nv.y, nv.z, vi.w);
             // binning of the new position
             int32_t cx, cy, cz;
             bin_cell(sd, np.x, np.y, np.z, cx, cy, cz);
-            const uint32_t c = sd.cell_base + local_cell(sd, cx, cy, cz);
-            v.key[pos] = c;
-            if (c != it.cell) {
-                const uint32_t t = tile_of(sd, cx, cy, cz);
-                if (t != item_tile) mark_occupied(v, t);
-            }
+            v.key[p] = sd.cell_base + local_cell(sd, cx, cy, cz);
+            mark_occupied(v, tile_of(sd, cx, cy, cz));
             if (spawn_scene) {
                 const uint32_t id = __float_as_uint(vi.w) - sd.id_base;
-                const float density = v.dens[pos];
+                const float density = v.dens[p];
                 // spawn_record's first test (shaders.js:806), checked inline
                 if (id < sd.n && density > 0.0f && density <= dv.gen->density_bubble_min)
                     spawn_eval(id, np, nv, q.w, density, sd, cmf + sd.cell_base, dv);
             }
         }
+        __syncthreads();
     }
 }
 
@@ -1221,19 +1288,15 @@ static void world_plan(World& w, uint32_t particle_cap, uint64_t cell_cap, uint3
     w.tile_cap = (uint32_t)(3 * (cell_cap / kTileCells)) + 64u * scene_cap + 64u;
     w.id_cap = particle_cap;
     w.scene_cap = scene_cap;
-    uint32_t off = 0;
-    w.cap_off[0] = 0;
-    for (int b = 1; b <= kMaxL; ++b) {
-        w.cap_off[b] = off;
-        off += w.npos / b + 1;
-    }
-    w.cap_off[kMaxL + 1] = off;
+    // every occupied tile has at most one partial chunk
+    w.chunk_cap = w.npos / kChunk + w.tile_cap + 1;
 }
 
 // Every device array of a world with its size (one list for allocation,
 // release and the footprint).
 template <class F> static void world_arrays(World& w, F&& f) {
     const size_t P = w.npos, C = w.cell_cap ? w.cell_cap : 1, T = w.tile_cap;
+    const size_t NG = (T + 1023) / 1024 + 1;
     for (int b = 0; b < 2; ++b) {
         f(w.posm[b], P * 16);
         f(w.velid[b], P * 16);
@@ -1242,16 +1305,19 @@ template <class F> static void world_arrays(World& w, F&& f) {
     }
     f(w.dens, P * 4);
     f(w.cell_count, (C + 1) * 4);
-    f(w.cell_info, C * 16);
-    f(w.bucket_items, (size_t)w.cap_off[kMaxL + 1] * 8);
+    f(w.cell_start, C * 4);
     f(w.key, P * 4);
     f(w.rank, P * 4);
     f(w.perm, P * 4);
     f(w.tile_flags, T * 4);
     f(w.tile_occ, T * 4);
-    f(w.tile_hist, (size_t)kMaxL * T * 4);
-    f(w.tile_base, (size_t)kMaxL * T * 4);
-    f(w.tile_chunk, (size_t)kMaxL * ((T + 1023) / 1024 + 1) * 4);
+    f(w.tile_cnt, T * 4);
+    f(w.tile_pstart, T * 4);
+    f(w.tile_cstart, T * 4);
+    f(w.group_pstart, NG * 4);
+    f(w.group_cstart, NG * 4);
+    f(w.chunk_info, (size_t)w.chunk_cap * 16);
+    f(w.chunk_last, (size_t)w.chunk_cap * 4);
     f(w.tile_occ_list, T * 4);
     f(w.tile_grid_list, T * 4);
     f(w.tile_scene, T * 4);
@@ -1284,7 +1350,7 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     w.sms = (uint32_t)sms;
-    w.item_blocks = (uint32_t)sms * 8;
+    w.item_blocks = (uint32_t)sms * 4;
     w.grid_blocks = (uint32_t)sms * 8;
     w.bin_blocks = (uint32_t)sms * 2;
     w.pos_blocks = std::min<uint32_t>(cdiv(w.npos, 256), (uint32_t)sms * 16);
@@ -1531,15 +1597,15 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
         k_tiles_occ<<<ntb, 256, 0, st>>>(v);
         k_bin_cells<<<w.bin_blocks, kTileCells, 0, st>>>(v);
         k_tiles_grid<<<ntb, 256, 0, st>>>(v);
-        k_tile_scan_local<<<dim3(v.nchunks, kMaxL), 1024, 0, st>>>(v);
-        k_tile_scan_chunks<<<kMaxL, 1024, 0, st>>>(v);
-        k_bucket_scan<<<1, 32, 0, st>>>(w.ctrl, gen_dev);
+        k_tile_scan_local<<<v.ngroups, 1024, 0, st>>>(v);
+        k_tile_scan_top<<<1, 1024, 0, st>>>(v, gen_dev);
+        k_tile_finish<<<w.bin_blocks, kTileCells, 0, st>>>(v);
         k_scatter<<<nposb, 256, 0, st>>>(v);
         w.launches += 8;
     }
     {
         Phase ph(prof, MPM_PHASE_P2G_MASS);
-        k_p2g_mass_items<<<w.item_blocks, kItemThreads, 0, st>>>(v, w.posm[cur], cm);
+        k_p2g_mass_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], cm);
         w.launches++;
     }
     {
@@ -1549,7 +1615,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     }
     {
         Phase ph(prof, MPM_PHASE_P2G_MOM);
-        k_p2g_mom_items<<<w.item_blocks, kItemThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.aff[cur], w.cmf, mv,
+        k_p2g_mom_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.aff[cur], w.cmf, mv,
                                                                 w.dens);
         w.launches++;
     }
@@ -1565,7 +1631,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     }
     {
         Phase ph(prof, MPM_PHASE_G2P);
-        k_g2p_items<<<w.item_blocks, kItemThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.mvf, w.cmf, w.posm[nxt],
+        k_g2p_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.mvf, w.cmf, w.posm[nxt],
                                                             w.velid[nxt], w.aff[nxt], dv);
         w.launches++;
     }
@@ -1573,11 +1639,11 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     w.gbuf ^= 1;
     w.cm_current = cm;
     w.dens_valid = true;
-    w.pos_bound = std::min<uint64_t>((uint64_t)w.n_total + kPosSlack, w.npos);
+    w.pos_bound = w.n_total;   // the layout after a substep is dense
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (dv.enabled) {
-        ds->diffuse.seed += 1u;   // mirrors the device-side bump in k_bucket_scan
+        ds->diffuse.seed += 1u;   // mirrors the device-side bump in k_tile_scan_top
         e = launch_diffuse(*ds, false);
     }
     return e;
@@ -1624,7 +1690,7 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
     if (e != cudaSuccess) return e;
     // host mirror of what the graph does
     w.launches += w.graph_kernels[p];
-    w.pos_bound = std::min<uint64_t>((uint64_t)w.n_total + kPosSlack, w.npos);
+    w.pos_bound = w.n_total;   // the layout after a substep is dense
     w.cm_current = w.grid_i32[w.gbuf];
     w.cur ^= 1;
     w.gbuf ^= 1;

@@ -3,7 +3,7 @@
 // A world holds any number of independent scenes (each its own grid, params
 // and walls) in shared device arrays: every scene owns a range of global
 // cells, a range of global tiles and a range of particle ids; particles of
-// all scenes share one position space, one set of length buckets and one
+// all scenes share one position space, one chunk list and one
 // launch per kernel per substep.  A single scene is a world of one.
 #pragma once
 
@@ -20,13 +20,26 @@ namespace mpm {
 constexpr int kTileX = 16, kTileY = 8, kTileZ = 8;
 constexpr int kTileCells = kTileX * kTileY * kTileZ;   // 1024: one thread per cell in k_bin_cells
 
-// A cell's particles are split into work items of at most kMaxL particles;
-// items are grouped by length into buckets 1..kMaxL so that the 32 lanes of a
-// warp always run the same number of iterations.
-constexpr int kMaxL = 16;
-// Positions lost to padding the last warp of each bucket: 31 * (1 + ... + kMaxL).
-constexpr uint32_t kPosSlack = 31u * (kMaxL * (kMaxL + 1) / 2) + 64u;
-constexpr uint32_t kHole = 0xFFFFFFFFu;   // key / id of a padding position
+// Particles are sorted by (tile, cell); each tile's particles are cut into
+// chunks of at most kChunk consecutive particles.  A chunk is one block's work
+// in the particle kernels: its cells form a box inside one tile, and the P2G
+// sums of the box plus a one-cell halo are accumulated in shared memory and
+// flushed to the grid once.
+#ifndef MPM_CHUNK
+#define MPM_CHUNK 512
+#endif
+#ifndef MPM_CHUNK_THREADS
+#define MPM_CHUNK_THREADS 256
+#endif
+constexpr uint32_t kChunk = MPM_CHUNK;
+constexpr int kChunkThreads = MPM_CHUNK_THREADS;
+static_assert(kChunk % kChunkThreads == 0, "a chunk is a whole number of passes of the block");
+// Largest halo box (a whole tile plus one cell on every side).
+constexpr int kHaloCells = (kTileX + 2) * (kTileY + 2) * (kTileZ + 2);
+// Positions of the layout beyond the particle count: none (the layout is
+// dense); the slack only rounds the position space.
+constexpr uint32_t kPosSlack = 256u;
+constexpr uint32_t kHole = 0xFFFFFFFFu;   // key / id of a position without a particle
 
 // Device scene table entry (read by the kernels).
 struct alignas(16) SceneDesc {
@@ -44,36 +57,36 @@ struct alignas(16) SceneDesc {
 // the start of every substep.
 struct Ctrl {
     uint32_t n_occ, n_grid, pad0, pad1;
-    uint32_t tail_cnt[kMaxL + 1];            // items of overpacked cells per length (unordered)
-    uint32_t pad2[64 - 4 - (kMaxL + 1)];
     // persistent
-    uint32_t bucket_reg[kMaxL + 2];          // ordered items per length (one per cell with 1..kMaxL particles)
-    uint32_t bucket_cnt[kMaxL + 2];          // ordered + tail items per length
-    uint32_t item_off[kMaxL + 2];            // first padded item index of each bucket
-    uint32_t pos_off[kMaxL + 2];             // first position of each bucket
-    uint32_t total_items, total_pos, prev_total_pos, pad3;
+    uint32_t total_chunks;      // chunks of the current layout
+    uint32_t total_pos;         // positions of the current layout
+    uint32_t prev_total_pos;    // positions of the previous layout (read through perm)
+    uint32_t pad2;
 };
-constexpr size_t kCtrlZeroBytes = 64 * 4;
+constexpr size_t kCtrlZeroBytes = 16;
 
 // Everything the device kernels need (passed by value).
 struct WorldView {
     uint32_t npos;             // capacity of the position space
     uint32_t ntiles;           // tiles in use (end of the allocated tile range)
-    uint32_t nchunks;          // ceil(ntiles / 1024): chunks of the two-level tile scan
-    uint32_t cap_off[kMaxL + 2];   // start of each bucket's item list in bucket_items
+    uint32_t ngroups;          // ceil(ntiles / 1024): groups of the two-level tile scan
+    uint32_t chunk_cap;        // capacity of the chunk list
     const SceneDesc* scenes;
     const uint32_t* tile_scene;    // scene of each global tile (kHole: free)
     uint32_t* cell_count;      // total cells + 1, zero outside binning
-    uint4* cell_info;          // per cell: (L | Llast<<8 | q<<16 | overpacked<<31, idx, idxLast|tile, scene)
-    uint2* bucket_items;       // (cell, scene) of each item, per bucket
+    uint32_t* cell_start;      // per cell: first position of its particles (local to the tile until finished)
     uint32_t* key;             // npos: binning cell (global) of each position of the current state, or kHole
     uint32_t* rank;            // npos: rank within the cell
     uint32_t* perm;            // npos: position -> position of the previous layout
     uint32_t* tile_flags;      // per tile
     uint32_t* tile_occ;        // per tile: 1 if the tile holds particles this substep
-    uint32_t* tile_hist;       // kMaxL x tiles: ordered items per (length, tile)
-    uint32_t* tile_base_;      // kMaxL x tiles: exclusive scan of tile_hist inside each 1024-tile chunk
-    uint32_t* tile_chunk;      // kMaxL x nchunks: exclusive scan of the chunk totals
+    uint32_t* tile_cnt;        // per tile: particles (occupied tiles)
+    uint32_t* tile_pstart;     // per tile: exclusive scan of tile_cnt inside its 1024-tile group
+    uint32_t* tile_cstart;     // per tile: exclusive scan of the chunk counts inside its group
+    uint32_t* group_pstart;    // per group: exclusive scan of the group particle totals
+    uint32_t* group_cstart;    // per group: exclusive scan of the group chunk totals
+    uint4* chunk_info;         // per chunk: (tile, first position, end position, first local cell)
+    uint32_t* chunk_last;      // per chunk: last local cell
     uint32_t* tile_occ_list;
     uint32_t* tile_grid_list;
     Ctrl* ctrl;
@@ -117,9 +130,8 @@ struct World {
     uint64_t cell_cap = 0;
     uint32_t tile_cap = 0, id_cap = 0, scene_cap = 0;
     uint32_t sms = 0;
-    uint32_t item_blocks = 0, grid_blocks = 0, bin_blocks = 0, pos_blocks = 0;
+    uint32_t item_blocks = 0, grid_blocks = 0, bin_blocks = 0, pos_blocks = 0;   // item_blocks: blocks of the chunk kernels
     uint64_t device_bytes = 0;              // device memory of the arrays below
-    uint32_t cap_off[kMaxL + 2] = {};
     std::vector<SceneRec> scenes;           // by scene slot
     RangeAlloc cells, tiles, ids;
     uint32_t n_total = 0;                   // particles in all scenes
@@ -141,16 +153,20 @@ struct World {
     float* aff[2] = {nullptr, nullptr};     // 9 planes of npos floats
     float* dens = nullptr;
     uint32_t* cell_count = nullptr;
-    uint4* cell_info = nullptr;
-    uint2* bucket_items = nullptr;
+    uint32_t* cell_start = nullptr;
     uint32_t* key = nullptr;
     uint32_t* rank = nullptr;
     uint32_t* perm = nullptr;
     uint32_t* tile_flags = nullptr;
     uint32_t* tile_occ = nullptr;
-    uint32_t* tile_hist = nullptr;
-    uint32_t* tile_base = nullptr;
-    uint32_t* tile_chunk = nullptr;
+    uint32_t* tile_cnt = nullptr;
+    uint32_t* tile_pstart = nullptr;
+    uint32_t* tile_cstart = nullptr;
+    uint32_t* group_pstart = nullptr;
+    uint32_t* group_cstart = nullptr;
+    uint4* chunk_info = nullptr;
+    uint32_t* chunk_last = nullptr;
+    uint32_t chunk_cap = 0;
     uint32_t* tile_occ_list = nullptr;
     uint32_t* tile_grid_list = nullptr;
     Ctrl* ctrl = nullptr;
