@@ -495,16 +495,27 @@ def served_comparison(local, rates=(50.0, 200.0, 2000.0), count=64, seed=0, budg
     return out
 
 
-def _profile_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if not os.path.exists(p):
+# kernel that carries each timed phase (for the DRAM traffic of its ncu summary)
+PHASE_KERNEL = {"p2g_mass": "k_p2g_mass_chunks", "p2g_mom": "k_p2g_mom_chunks", "g2p": "k_g2p_chunks",
+                "update_grid": "k_update_tiles"}
+
+
+def _profile_traffic(phase, workload=WORKLOAD):
+    """DRAM bytes (read + write) per launch of the phase's kernel, from the
+    `dram_bytes_per_launch <kernel> <workload> <bytes>` lines of the committed
+    ncu summaries under profiles/, or None."""
+    kernel = PHASE_KERNEL.get(phase)
+    d = os.path.join(ROOT, "profiles")
+    if not kernel or not os.path.isdir(d):
         return None
-    try:
-        d = json.load(open(p))
-        return d.get(WORKLOAD, {}).get(kernel)
-    except Exception:
-        return None
+    for f in sorted(os.listdir(d)):
+        if not f.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(d, f)):
+            parts = line.split()
+            if len(parts) == 4 and parts[0] == "dram_bytes_per_launch" and parts[1] == kernel and parts[2] == workload:
+                return int(parts[3])
+    return None
 
 
 if __name__ == "__main__":
