@@ -448,13 +448,6 @@ __device__ __forceinline__ PW particle_weights(float px, float py, float pz) {
     return w;
 }
 
-__device__ __forceinline__ void cell_xyz(const SceneDesc& sd, uint32_t gc, int32_t& x, int32_t& y, int32_t& z) {
-    const uint32_t c = gc - sd.cell_base;
-    x = (int32_t)(c % sd.X);
-    y = (int32_t)((c / sd.X) % sd.Y);
-    z = (int32_t)(c / (sd.X * sd.Y));
-}
-
 // encode() without the clamp, for values already known to lie in +-20000.
 __device__ __forceinline__ int32_t encode_unclamped(float v) { return __float2int_rz(v * kFixed); }
 
@@ -532,10 +525,27 @@ __device__ __forceinline__ bool in_halo(const PW& w, const ChunkHdr& h, const Sc
            w.cx + 1 < (int32_t)sd.X && w.cy + 1 < (int32_t)sd.Y && w.cz + 1 < (int32_t)sd.Z;
 }
 
-// Scene-local cell of halo index i, or false when it lies outside the grid.
-__device__ __forceinline__ bool halo_cell(const ChunkHdr& h, const SceneDesc& sd, int i, uint32_t& cell) {
-    const int hxy = h.hx * h.hy;
-    const int32_t x = h.ox + i % h.hx, y = h.oy + (i / h.hx) % h.hy, z = h.oz + i / hxy;
+// Shared halo arrays use the strides of the largest box (a tile plus its
+// halo) whatever the chunk's box, so the 27 stencil offsets of a particle are
+// compile-time constants.
+constexpr int kHX = kTileX + 2, kHXY = (kTileX + 2) * (kTileY + 2);
+static_assert(kHXY * (kTileZ + 2) == kHaloCells, "halo strides");
+
+// Halo slot of the stencil base (cx-1, cy-1, cz-1).
+__device__ __forceinline__ int halo_base(const ChunkHdr& h, int32_t cx, int32_t cy, int32_t cz) {
+    return (cz - 1 - h.oz) * kHXY + (cy - 1 - h.oy) * kHX + (cx - 1 - h.ox);
+}
+
+// Slots of the halo arrays that the chunk's box spans: [0, halo_span(h)).
+// Loops over them divide by compile-time strides only.
+__device__ __forceinline__ int halo_span(const ChunkHdr& h) { return h.hz * kHXY; }
+
+// Slot s as a cell of the chunk's box inside the grid: its scene-local cell,
+// or false for a slot outside the box or a box cell outside the grid.
+__device__ __forceinline__ bool halo_cell(const ChunkHdr& h, const SceneDesc& sd, int s, uint32_t& cell) {
+    const int dz = s / kHXY, r = s - dz * kHXY, dy = r / kHX, dx = r - dy * kHX;
+    if (dx >= h.hx || dy >= h.hy) return false;
+    const int32_t x = h.ox + dx, y = h.oy + dy, z = h.oz + dz;
     if (x < 0 || y < 0 || z < 0 || x >= (int32_t)sd.X || y >= (int32_t)sd.Y || z >= (int32_t)sd.Z) return false;
     cell = local_cell(sd, x, y, z);
     return true;
@@ -590,7 +600,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             const uint32_t p = h.first + r * kChunkThreads + chunk_lane_offset();
             q[r] = p < h.end ? posm[v.perm[p]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
-        const int hn = h.hx * h.hy * h.hz, hxy = h.hx * h.hy;
+        const int hn = halo_span(h);
         for (int i = threadIdx.x; i < hn; i += blockDim.x) acc[i] = 0;
         __syncthreads();
         const SceneDesc& sd = v.scenes[h.scene];
@@ -599,7 +609,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             const bool valid = h.first + r * kChunkThreads + chunk_lane_offset() < h.end;
             const PW w = particle_weights(q[r].x, q[r].y, q[r].z);
             const bool fast = valid && in_halo(w, h, sd);
-            const int hb = ((w.cz - 1 - h.oz) * h.hy + (w.cy - 1 - h.oy)) * h.hx + (w.cx - 1 - h.ox);
+            const int hb = halo_base(h, w.cx, w.cy, w.cz);
             bool leader;
             const uint32_t grp = agg_group(fast, hb, lane, leader);
             if (fast) {
@@ -613,7 +623,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
                         for (int i = 0; i < 3; ++i) {
                             const float x = w.wx[i] * w.wy[j] * w.wz[kk] * q[r].w;
                             const int32_t e = safe ? encode_unclamped(x) : encode(x);
-                            agg_add(&acc[hb + kk * hxy + j * h.hx + i], e, grp, leader);
+                            agg_add(&acc[hb + kk * kHXY + j * kHX + i], e, grp, leader);
                         }
             } else if (valid) {
                 // stencil outside the halo or the grid: bounds-checked global atomics
@@ -824,11 +834,10 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
                                              const float* mh, int32_t (*acc)[kHaloCells],
                                              const float* __restrict__ scmf, int32_t* __restrict__ smv,
                                              float* __restrict__ dens, uint32_t lane) {
-    const int hxy = h.hx * h.hy;
     const uint32_t X = sd.X, SLICE = sd.X * sd.Y, G = sd.G;
     const PW w = particle_weights(pm.x, pm.y, pm.z);
     const bool fast = valid && in_halo(w, h, sd);
-    const int hb = ((w.cz - 1 - h.oz) * h.hy + (w.cy - 1 - h.oy)) * h.hx + (w.cx - 1 - h.ox);
+    const int hb = halo_base(h, w.cx, w.cy, w.cz);
     const uint32_t baseIdx = (uint32_t)(((w.cz - 1) * (int32_t)sd.Y + (w.cy - 1)) * (int32_t)X + (w.cx - 1));
     // density (shaders.js:305-313), k, j, i order
     float density = 0.0f;
@@ -839,7 +848,7 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
             for (int jj = 0; jj < 3; ++jj)
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
-                    density += w.wx[i] * w.wy[jj] * w.wz[k] * mh[hb + k * hxy + jj * h.hx + i];
+                    density += w.wx[i] * w.wy[jj] * w.wz[k] * mh[hb + k * kHXY + jj * kHX + i];
     } else if (valid) {
         for (int k = 0; k < 3; ++k)
             for (int jj = 0; jj < 3; ++jj)
@@ -882,7 +891,7 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
     const uint32_t grp = agg_group(shared_path, hb, lane, leader);
     if (shared_path) {
         auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
-            const int hi = hb + k * hxy + j * h.hx + i;
+            const int hi = hb + k * kHXY + j * kHX + i;
             agg_add(&acc[0][hi], ex, grp, leader);
             agg_add(&acc[1][hi], ey, grp, leader);
             agg_add(&acc[2][hi], ez, grp, leader);
@@ -903,6 +912,9 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
     }
 }
 
+#ifndef MPM_G2P_MINB
+#define MPM_G2P_MINB 4
+#endif
 #ifndef MPM_MOM_PREFETCH
 #define MPM_MOM_PREFETCH 1
 #endif
@@ -947,7 +959,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
 #pragma unroll
             for (int e = 0; e < 9; ++e) a[e] = valid ? aff[e * plane + slot] : 0.0f;
         }
-        const int hn = h.hx * h.hy * h.hz;
+        const int hn = halo_span(h);
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
             uint32_t cell;
             mh[i] = halo_cell(h, sd, i, cell) ? scmf[cell] : 0.0f;
@@ -1032,9 +1044,19 @@ __device__ __forceinline__ bool estimate_normal_f(const float* __restrict__ cmf,
 
 // Spawn decision + staging (shaders.js:800-855), out of line: most particles
 // fail the density test that the caller applies first.
-__device__ __noinline__ void spawn_eval(uint32_t id, f3 np, f3 nv, float m, float density, const SceneDesc& sd,
-                                        const float* __restrict__ cmf, const DiffuseView& dv) {
-    const mpm_gen_params& gen = *dv.gen;
+#ifndef MPM_G2P_RARE_INLINE
+#define MPM_G2P_RARE_INLINE 0
+#endif
+#if MPM_G2P_RARE_INLINE
+#define MPM_G2P_RARE __forceinline__
+#else
+#define MPM_G2P_RARE __noinline__
+#endif
+__device__ MPM_G2P_RARE void spawn_eval(uint32_t id, f3 np, f3 nv, float m, float density, const SceneDesc& sd,
+                                        const float* __restrict__ cmf, const mpm_gen_params* __restrict__ genp,
+                                        mpm_diffuse_particle* __restrict__ staging,
+                                        uint32_t* __restrict__ spawn_bits) {
+    const mpm_gen_params& gen = *genp;
     const f3 vel = nv;
     const float speed2 = dot3(vel, vel);
     const float speed = __fsqrt_rn(speed2);
@@ -1069,8 +1091,8 @@ __device__ __noinline__ void spawn_eval(uint32_t id, f3 np, f3 nv, float m, floa
     r.pos[0] = np.x; r.pos[1] = np.y; r.pos[2] = np.z; r.pos[3] = 0.0f;
     r.vel[0] = vel.x + jx; r.vel[1] = vel.y + jy; r.vel[2] = vel.z + jz; r.vel[3] = 0.0f;
     r.ptype = ptype; r.alive = 1u; r.lifetime = lifetime; r._pad = 0.0f;
-    dv.staging[id] = r;
-    atomicOr(&dv.spawn_bits[id >> 5], 1u << (id & 31u));
+    staging[id] = r;
+    atomicOr(&spawn_bits[id >> 5], 1u << (id & 31u));
 }
 
 // G2P for one particle given its gathered grid velocity (shaders.js:636-700).
@@ -1122,9 +1144,23 @@ __device__ __forceinline__ void g2p_finish(const float4 q, float gvx, float gvy,
 
 // G2P gather for a particle whose stencil leaves the halo box or the grid:
 // the reference's linear stencil index with a bounds guard.
-__device__ __noinline__ void g2p_gather_direct(const PW& w, const float4 q, const float* __restrict__ mvf, uint32_t X,
-                                               uint32_t Y, uint32_t G, float& gvx, float& gvy, float& gvz,
-                                               float* B) {
+struct G2PSum {
+    float gv[3];
+    float B[9];
+};
+
+// Returned by value: a pointer to the caller's accumulators would keep them
+// in local memory on the common (halo) path too.
+__device__ MPM_G2P_RARE G2PSum g2p_gather_direct(const PW w, const float4 q, const float* __restrict__ mvf,
+                                                 uint32_t X, uint32_t Y, uint32_t G) {
+    G2PSum r;
+    float& gvx = r.gv[0];
+    float& gvy = r.gv[1];
+    float& gvz = r.gv[2];
+    float* B = r.B;
+    gvx = gvy = gvz = 0.0f;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) B[e] = 0.0f;
     const uint32_t SLICE = X * Y;
     const int32_t bx = w.cx - 1, by = w.cy - 1, bz = w.cz - 1;
     const uint32_t baseIdx = (uint32_t)((bz * (int32_t)Y + by) * (int32_t)X + bx);
@@ -1151,10 +1187,63 @@ __device__ __noinline__ void g2p_gather_direct(const PW& w, const float4 q, cons
             }
         }
     }
+    return r;
 }
 
 
-__global__ void __launch_bounds__(kChunkThreads) k_g2p_chunks(WorldView v, const float4* __restrict__ posm,
+// Where G2P writes: the new state, the binning key and tile marks, and the
+// diffuse spawn staging.
+struct G2POut {
+    float4* posm;
+    float4* velid;
+    float* aff;
+    size_t plane;
+    uint32_t* key;
+    uint32_t* tile_flags;
+    const float* dens;
+    const float* cmf;                    // scene's decoded cell masses
+    const mpm_gen_params* gen;           // null: no spawning for this scene
+    mpm_diffuse_particle* staging;
+    uint32_t* spawn_bits;
+};
+
+// G2P epilogue of one particle (shaders.js:631-700): affine, advection and
+// boundary handling, the new state at position p, its binning key and tile
+// mark, and the diffuse spawn decision.
+__device__ __forceinline__ void g2p_store(const G2POut& o, const SceneDesc& sd, uint32_t p, const float4 q,
+                                          const float4 vi, float gvx, float gvy, float gvz, const float* B) {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) o.aff[e * o.plane + p] = B[e] * 4.0f;
+    f3 np, nv;
+    g2p_finish(q, gvx, gvy, gvz, sd.P, sd.W, np, nv);
+    o.posm[p] = make_float4(np.x, np.y, np.z, q.w);
+    o.velid[p] = make_float4(nv.x, nv.y, nv.z, vi.w);
+    // binning of the new position
+    int32_t cx, cy, cz;
+    bin_cell(sd, np.x, np.y, np.z, cx, cy, cz);
+    o.key[p] = sd.cell_base + local_cell(sd, cx, cy, cz);
+    const uint32_t t = tile_of(sd, cx, cy, cz);
+    if ((o.tile_flags[t] & 1u) == 0u) atomicOr(&o.tile_flags[t], 1u);
+    if (o.gen) {
+        const uint32_t id = __float_as_uint(vi.w) - sd.id_base;
+        const float density = o.dens[p];
+        // spawn_record's first test (shaders.js:806), checked inline
+        if (id < sd.n && density > 0.0f && density <= o.gen->density_bubble_min)
+            spawn_eval(id, np, nv, q.w, density, sd, o.cmf, o.gen, o.staging, o.spawn_bits);
+    }
+}
+
+// G2P of a particle whose stencil leaves the halo box or the grid (rare): the
+// reference's linear stencil index with a bounds guard, then the epilogue.
+__device__ __noinline__ void g2p_direct_particle(const G2POut o, const SceneDesc* sdp, uint32_t p, const float4 q,
+                                                 const float4 vi, const float* __restrict__ mvf) {
+    const SceneDesc& sd = *sdp;
+    const PW w = particle_weights(q.x, q.y, q.z);
+    const G2PSum r = g2p_gather_direct(w, q, mvf, sd.X, sd.Y, sd.G);
+    g2p_store(o, sd, p, q, vi, r.gv[0], r.gv[1], r.gv[2], r.B);
+}
+
+__global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(WorldView v, const float4* __restrict__ posm,
                                                               const float4* __restrict__ velid,
                                                               const float* __restrict__ mvf,
                                                               const float* __restrict__ cmf,
@@ -1188,7 +1277,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_g2p_chunks(WorldView v, const
             }
         }
 #endif
-        const int hn = h.hx * h.hy * h.hz, hxy = h.hx * h.hy;
+        const int hn = halo_span(h);
         const float* smvf = mvf + 3ull * sd.cell_base;
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
             uint32_t cell;
@@ -1205,7 +1294,8 @@ __global__ void __launch_bounds__(kChunkThreads) k_g2p_chunks(WorldView v, const
         }
         __syncthreads();
         const bool spawn_scene = dv.enabled && h.scene == dv.scene;
-        const uint32_t X = sd.X, G = sd.G;
+        const G2POut out{posm_out, velid_out, aff_out, plane, v.key, v.tile_flags, v.dens, cmf + sd.cell_base,
+                         spawn_scene ? dv.gen : nullptr, dv.staging, dv.spawn_bits};
 #pragma unroll 1
         for (int r = 0; r < kPer; ++r) {
             const uint32_t p = h.first + r * kChunkThreads + threadIdx.x;
@@ -1219,11 +1309,15 @@ __global__ void __launch_bounds__(kChunkThreads) k_g2p_chunks(WorldView v, const
             const float4 vi = velid[slot];
 #endif
             const PW w = particle_weights(q.x, q.y, q.z);
+            if (!in_halo(w, h, sd)) {
+                g2p_direct_particle(out, &sd, p, q, vi, smvf);
+                continue;
+            }
             float gvx = 0.0f, gvy = 0.0f, gvz = 0.0f;
             float B[9] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-            if (in_halo(w, h, sd)) {
+            {
                 const int32_t bx = w.cx - 1, by = w.cy - 1, bz = w.cz - 1;
-                const int hb = ((bz - h.oz) * h.hy + (by - h.oy)) * h.hx + (bx - h.ox);
+                const int hb = halo_base(h, w.cx, w.cy, w.cz);
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     const float wzk = w.wz[k];
@@ -1236,7 +1330,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_g2p_chunks(WorldView v, const
                         for (int i = 0; i < 3; ++i) {
                             const float ww = w.wx[i] * wyzk;
                             const float dxi = __int2float_rn(bx + i) - q.x + 0.5f;
-                            const int hi = hb + k * hxy + jj * h.hx + i;
+                            const int hi = hb + k * kHXY + jj * kHX + i;
                             const float wvx = ww * vh[0][hi], wvy = ww * vh[1][hi], wvz = ww * vh[2][hi];
                             gvx += wvx; gvy += wvy; gvz += wvz;
                             B[0] += wvx * dxi; B[1] += wvx * dyj; B[2] += wvx * dzk;
@@ -1245,27 +1339,8 @@ __global__ void __launch_bounds__(kChunkThreads) k_g2p_chunks(WorldView v, const
                         }
                     }
                 }
-            } else {
-                g2p_gather_direct(w, q, smvf, X, sd.Y, G, gvx, gvy, gvz, B);
             }
-#pragma unroll
-            for (int e = 0; e < 9; ++e) aff_out[e * plane + p] = B[e] * 4.0f;
-            f3 np, nv;
-            g2p_finish(q, gvx, gvy, gvz, sd.P, sd.W, np, nv);
-            posm_out[p] = make_float4(np.x, np.y, np.z, q.w);
-            velid_out[p] = make_float4(nv.x, nv.y, nv.z, vi.w);
-            // binning of the new position
-            int32_t cx, cy, cz;
-            bin_cell(sd, np.x, np.y, np.z, cx, cy, cz);
-            v.key[p] = sd.cell_base + local_cell(sd, cx, cy, cz);
-            mark_occupied(v, tile_of(sd, cx, cy, cz));
-            if (spawn_scene) {
-                const uint32_t id = __float_as_uint(vi.w) - sd.id_base;
-                const float density = v.dens[p];
-                // spawn_record's first test (shaders.js:806), checked inline
-                if (id < sd.n && density > 0.0f && density <= dv.gen->density_bubble_min)
-                    spawn_eval(id, np, nv, q.w, density, sd, cmf + sd.cell_base, dv);
-            }
+            g2p_store(out, sd, p, q, vi, gvx, gvy, gvz, B);
         }
         __syncthreads();
     }
