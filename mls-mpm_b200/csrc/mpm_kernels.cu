@@ -438,17 +438,6 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_gen_eval(const float4* __r
     }
 }
 
-// Popcount of each group of kGroupIds ids (8 words; one thread per word).
-__global__ void __launch_bounds__(256) k_group_counts(const uint32_t* __restrict__ bits, uint32_t nwords,
-                                                      uint32_t* __restrict__ counts) {
-    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t c = w < nwords ? __popc(bits[w]) : 0u;
-    c += __shfl_xor_sync(0xffffffffu, c, 1);
-    c += __shfl_xor_sync(0xffffffffu, c, 2);
-    c += __shfl_xor_sync(0xffffffffu, c, 4);
-    if ((w & 7u) == 0u && w < nwords) counts[w >> 3] = c;
-}
-
 // Exclusive scan of the group counts (one block).  Applies the pass to the
 // free-list top: mode 0 (spawn) pops min(total, top) slots when top > 0,
 // mode 1 (kill) pushes total slots.  state = {top before, total, applied}.
@@ -502,31 +491,41 @@ __global__ void __launch_bounds__(1024) k_rank_scan(uint32_t* __restrict__ count
     }
 }
 
-// Rank of set bit `id` among the set bits (ascending id).
-__device__ __forceinline__ uint32_t bit_rank(const uint32_t* __restrict__ bits, uint32_t word, uint32_t id,
-                                             const uint32_t* __restrict__ group_offsets) {
-    const uint32_t w = id >> 5;
-    uint32_t r = group_offsets[id / kGroupIds] + __popc(word & ((1u << (id & 31u)) - 1u));
-    for (uint32_t k = w & ~7u; k < w; ++k) r += __popc(bits[k]);
-    return r;
+// Rank of this thread's bit among the set bits of its group (kGroupIds ids,
+// one per thread of a 256-thread block; warp k holds word k of the group),
+// in ascending id order.  bit: whether this thread's bit is set.
+__device__ __forceinline__ uint32_t group_bit_rank(uint32_t word, bool& bit) {
+    __shared__ uint32_t wc[kGroupIds / 32];
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    if (lane == 0) wc[wid] = __popc(word);
+    __syncthreads();
+    uint32_t pre = 0;
+    for (uint32_t k = 0; k < wid; ++k) pre += wc[k];
+    bit = (word >> lane) & 1u;
+    return pre + __popc(word & ((1u << lane) - 1u));
 }
 
-// Spawner of rank r takes free_list[top-1-r] if r < applied (one thread per id).
-__global__ void __launch_bounds__(256) k_spawn_write(const uint32_t* __restrict__ bits, uint32_t n,
-                                                     const uint32_t* __restrict__ counts,
-                                                     const int32_t* __restrict__ state,
-                                                     const uint32_t* __restrict__ free_list,
-                                                     const mpm_diffuse_particle* __restrict__ staging,
-                                                     mpm_diffuse_particle* __restrict__ pool, uint32_t M) {
-    const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= n) return;
-    const uint32_t word = bits[id >> 5];
-    if (!((word >> (id & 31u)) & 1u)) return;
-    const uint32_t r = bit_rank(bits, word, id, counts);
+// Spawners in ascending id take free-list slots top-1, top-2, ...: the
+// spawner of rank r takes free_list[top-1-r] if r < applied.  One block per
+// group of kGroupIds ids (counts: exclusive group offsets from k_rank_scan,
+// state[1] the total); groups without spawners return at once.
+__global__ void __launch_bounds__(kGroupIds) k_spawn_write(const uint32_t* __restrict__ bits, uint32_t n,
+                                                           const uint32_t* __restrict__ counts,
+                                                           const int32_t* __restrict__ state,
+                                                           const uint32_t* __restrict__ free_list,
+                                                           const mpm_diffuse_particle* __restrict__ staging,
+                                                           mpm_diffuse_particle* __restrict__ pool, uint32_t M) {
+    const uint32_t g = blockIdx.x, ng = (n + kGroupIds - 1) / kGroupIds;
+    const uint32_t c0 = counts[g], c1 = g + 1 < ng ? counts[g + 1] : (uint32_t)state[1];
     const int32_t t0 = state[0], applied = state[2];
+    if (c1 == c0 || (int32_t)c0 >= applied) return;   // block-uniform
+    const uint32_t id = g * kGroupIds + threadIdx.x;
+    const uint32_t word = id < n ? bits[id >> 5] : 0u;   // the bitmap holds ceil(n/32) words
+    bool bit;
+    const uint32_t r = c0 + group_bit_rank(word, bit);
     const int32_t fi = t0 - 1 - (int32_t)r;
     // free-list state uploaded by a caller may be inconsistent: never index outside the pool
-    if ((int32_t)r < applied && fi >= 0 && (uint32_t)fi < M) {
+    if (bit && id < n && (int32_t)r < applied && fi >= 0 && (uint32_t)fi < M) {
         const uint32_t slot = free_list[fi];
         if (slot < M) pool[slot] = staging[id];
     }
@@ -658,18 +657,22 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particl
     }
 }
 
-// Killed slot of rank r goes to free_list[top + r] (one thread per slot).
-__global__ void __launch_bounds__(256) k_kill_push(const uint32_t* __restrict__ bits, uint32_t M,
-                                                   const uint32_t* __restrict__ counts,
-                                                   const int32_t* __restrict__ state,
-                                                   uint32_t* __restrict__ free_list) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M) return;
-    const uint32_t word = bits[i >> 5];
-    if (!((word >> (i & 31u)) & 1u)) return;
-    const uint32_t r = bit_rank(bits, word, i, counts);
+// Killed slots in ascending order go to free_list[top], free_list[top+1], ...
+// One block per group of kGroupIds slots (counts: exclusive group offsets,
+// state[1] the total); groups without kills return at once.
+__global__ void __launch_bounds__(kGroupIds) k_kill_push(const uint32_t* __restrict__ bits, uint32_t M,
+                                                         const uint32_t* __restrict__ counts,
+                                                         const int32_t* __restrict__ state,
+                                                         uint32_t* __restrict__ free_list) {
+    const uint32_t g = blockIdx.x, ng = (M + kGroupIds - 1) / kGroupIds;
+    const uint32_t c0 = counts[g], c1 = g + 1 < ng ? counts[g + 1] : (uint32_t)state[1];
+    if (c1 == c0) return;   // block-uniform
+    const uint32_t i = g * kGroupIds + threadIdx.x;
+    const uint32_t word = i < M ? bits[i >> 5] : 0u;   // the bitmap holds ceil(M/32) words
+    bool bit;
+    const uint32_t r = c0 + group_bit_rank(word, bit);
     const int32_t fi = state[0] + (int32_t)r;
-    if (fi >= 0 && (uint32_t)fi < M) free_list[fi] = i;
+    if (bit && i < M && fi >= 0 && (uint32_t)fi < M) free_list[fi] = i;
 }
 
 cudaError_t launch_apply_hand(Scene& s) {
@@ -697,13 +700,13 @@ cudaError_t launch_diffuse(Scene& s, bool eval) {
             gen.seed = d.seed;
             k_diffuse_gen_eval<<<ng, kThreads, 0, st>>>(s.pos, s.vel, s.mass, s.dens, s.cmf, P, gen, d.staging,
                                                         d.spawn_bits, d.block_counts);
-        } else {
-            k_group_counts<<<blocks_for(nwords, 256), 256, 0, st>>>(d.spawn_bits, nwords, d.block_counts);
+            s.launches++;
         }
+        // (the binned engine's G2P has already counted the spawners per group)
         k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, ng, d.top, d.rank_state, 0);
-        k_spawn_write<<<ng, 256, 0, st>>>(d.spawn_bits, n, d.block_counts, d.rank_state, d.free_list, d.staging,
-                                          d.pool, d.max_count);
-        s.launches += 3;
+        k_spawn_write<<<ng, kGroupIds, 0, st>>>(d.spawn_bits, n, d.block_counts, d.rank_state, d.free_list,
+                                                d.staging, d.pool, d.max_count);
+        s.launches += 2;
     } else if (eval) {
         d.seed = d.seed + 1u;
     }
@@ -715,7 +718,7 @@ cudaError_t launch_diffuse(Scene& s, bool eval) {
         Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
         k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, P, adv, s.walls, d.kill_bits, d.block_counts);
         k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mg, d.top, d.rank_state, 1);
-        k_kill_push<<<mg, 256, 0, st>>>(d.kill_bits, M, d.block_counts, d.rank_state, d.free_list);
+        k_kill_push<<<mg, kGroupIds, 0, st>>>(d.kill_bits, M, d.block_counts, d.rank_state, d.free_list);
         s.launches += 3;
     }
     return cudaGetLastError();

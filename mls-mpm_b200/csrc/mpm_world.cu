@@ -1055,7 +1055,7 @@ __device__ __forceinline__ bool estimate_normal_f(const float* __restrict__ cmf,
 __device__ MPM_G2P_RARE void spawn_eval(uint32_t id, f3 np, f3 nv, float m, float density, const SceneDesc& sd,
                                         const float* __restrict__ cmf, const mpm_gen_params* __restrict__ genp,
                                         mpm_diffuse_particle* __restrict__ staging,
-                                        uint32_t* __restrict__ spawn_bits) {
+                                        uint32_t* __restrict__ spawn_bits, uint32_t* __restrict__ group_counts) {
     const mpm_gen_params& gen = *genp;
     const f3 vel = nv;
     const float speed2 = dot3(vel, vel);
@@ -1093,6 +1093,7 @@ __device__ MPM_G2P_RARE void spawn_eval(uint32_t id, f3 np, f3 nv, float m, floa
     r.ptype = ptype; r.alive = 1u; r.lifetime = lifetime; r._pad = 0.0f;
     staging[id] = r;
     atomicOr(&spawn_bits[id >> 5], 1u << (id & 31u));
+    atomicAdd(&group_counts[id / kGroupIds], 1u);
 }
 
 // G2P for one particle given its gathered grid velocity (shaders.js:636-700).
@@ -1199,12 +1200,15 @@ struct G2POut {
     float* aff;
     size_t plane;
     uint32_t* key;
+    uint32_t* rank;
+    uint32_t* cell_count;
     uint32_t* tile_flags;
     const float* dens;
     const float* cmf;                    // scene's decoded cell masses
     const mpm_gen_params* gen;           // null: no spawning for this scene
     mpm_diffuse_particle* staging;
     uint32_t* spawn_bits;
+    uint32_t* group_counts;
 };
 
 // G2P epilogue of one particle (shaders.js:631-700): affine, advection and
@@ -1221,7 +1225,10 @@ __device__ __forceinline__ void g2p_store(const G2POut& o, const SceneDesc& sd, 
     // binning of the new position
     int32_t cx, cy, cz;
     bin_cell(sd, np.x, np.y, np.z, cx, cy, cz);
-    o.key[p] = sd.cell_base + local_cell(sd, cx, cy, cz);
+    const uint32_t key = sd.cell_base + local_cell(sd, cx, cy, cz);
+    o.key[p] = key;
+    // the rank within the cell for the next substep's binning (k_count's work)
+    o.rank[p] = atomicAdd(&o.cell_count[key], 1u);
     const uint32_t t = tile_of(sd, cx, cy, cz);
     if ((o.tile_flags[t] & 1u) == 0u) atomicOr(&o.tile_flags[t], 1u);
     if (o.gen) {
@@ -1229,7 +1236,7 @@ __device__ __forceinline__ void g2p_store(const G2POut& o, const SceneDesc& sd, 
         const float density = o.dens[p];
         // spawn_record's first test (shaders.js:806), checked inline
         if (id < sd.n && density > 0.0f && density <= o.gen->density_bubble_min)
-            spawn_eval(id, np, nv, q.w, density, sd, o.cmf, o.gen, o.staging, o.spawn_bits);
+            spawn_eval(id, np, nv, q.w, density, sd, o.cmf, o.gen, o.staging, o.spawn_bits, o.group_counts);
     }
 }
 
@@ -1294,8 +1301,9 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         }
         __syncthreads();
         const bool spawn_scene = dv.enabled && h.scene == dv.scene;
-        const G2POut out{posm_out, velid_out, aff_out, plane, v.key, v.tile_flags, v.dens, cmf + sd.cell_base,
-                         spawn_scene ? dv.gen : nullptr, dv.staging, dv.spawn_bits};
+        const G2POut out{posm_out, velid_out, aff_out, plane, v.key, v.rank, v.cell_count, v.tile_flags, v.dens,
+                         cmf + sd.cell_base,
+                         spawn_scene ? dv.gen : nullptr, dv.staging, dv.spawn_bits, dv.group_counts};
 #pragma unroll 1
         for (int r = 0; r < kPer; ++r) {
             const uint32_t p = h.first + r * kChunkThreads + threadIdx.x;
@@ -1564,6 +1572,7 @@ cudaError_t world_add_scene(World& w, uint32_t X, uint32_t Y, uint32_t Z, const 
     r.id_base = (uint32_t)ib; r.n = n; r.id_cap = n ? n : 1;
     world_set_uniforms(w, slot, P, W, nullptr, 0, nullptr);
     w.generation++;
+    w.counted = false;
     for (uint32_t t = 0; t < nt; ++t) w.h_tile_scene[tb + t] = (uint32_t)slot;
     e = cudaMemcpyAsync(w.tile_scene + tb, w.h_tile_scene.data() + tb, (size_t)nt * 4, cudaMemcpyHostToDevice,
                         w.stream);
@@ -1626,6 +1635,7 @@ cudaError_t world_remove_scene(World& w, int slot) {
     r = SceneRec();
     w.table_dirty = true;
     w.generation++;
+    w.counted = false;
     if (e == cudaSuccess) e = cudaGetLastError();
     return e;
 }
@@ -1660,6 +1670,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
         dv.gen = ds->diffuse.gen_dev;
         dv.staging = ds->diffuse.staging;
         dv.spawn_bits = ds->diffuse.spawn_bits;
+        dv.group_counts = ds->diffuse.block_counts;
         gen_dev = ds->diffuse.gen_dev;
     }
     Scene* prof = ds;
@@ -1668,7 +1679,13 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
         Phase ph(prof, MPM_PHASE_SORT);
         e = cudaMemsetAsync(w.ctrl, 0, kCtrlZeroBytes, st);
         if (e != cudaSuccess) return e;
-        k_count<<<nposb, 256, 0, st>>>(v);
+        if (!w.counted) {
+            // scenes were added or removed since the last G2P counted: recount
+            e = cudaMemsetAsync(w.cell_count, 0, ((size_t)w.cell_cap + 1) * 4, st);
+            if (e != cudaSuccess) return e;
+            k_count<<<nposb, 256, 0, st>>>(v);
+            w.launches++;
+        }
         k_tiles_occ<<<ntb, 256, 0, st>>>(v);
         k_bin_cells<<<w.bin_blocks, kTileCells, 0, st>>>(v);
         k_tiles_grid<<<ntb, 256, 0, st>>>(v);
@@ -1676,7 +1693,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
         k_tile_scan_top<<<1, 1024, 0, st>>>(v, gen_dev);
         k_tile_finish<<<w.bin_blocks, kTileCells, 0, st>>>(v);
         k_scatter<<<nposb, 256, 0, st>>>(v);
-        w.launches += 8;
+        w.launches += 7;
     }
     {
         Phase ph(prof, MPM_PHASE_P2G_MASS);
@@ -1703,6 +1720,8 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
         const uint32_t n = w.scenes[dv.scene].n;
         e = cudaMemsetAsync(dv.spawn_bits, 0, ((size_t)(n + 31) / 32) * 4, st);
         if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(dv.group_counts, 0, ((size_t)(n + kGroupIds - 1) / kGroupIds) * 4, st);
+        if (e != cudaSuccess) return e;
     }
     {
         Phase ph(prof, MPM_PHASE_G2P);
@@ -1714,6 +1733,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     w.gbuf ^= 1;
     w.cm_current = cm;
     w.dens_valid = true;
+    w.counted = true;   // G2P ranked every new position in its cell
     w.pos_bound = w.n_total;   // the layout after a substep is dense
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1729,7 +1749,8 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
     if (e != cudaSuccess) return e;
     const bool diffuse = ds && ds->diffuse.enabled;
     const bool profiling = ds && ds->profile;
-    if (!use_graph || diffuse || profiling) return enqueue_substep(w, ds);
+    // a substep that must recount runs eagerly; the captured graphs never count
+    if (!use_graph || diffuse || profiling || !w.counted) return enqueue_substep(w, ds);
     const int p = w.cur;   // cur and gbuf flip together: one graph per parity
     if (!w.graph[p] || w.graph_gen[p] != w.generation) {
         if (w.graph[p]) {

@@ -100,6 +100,7 @@ struct DiffuseView {
     const mpm_gen_params* gen;       // device copy; seed bumped on the device each substep
     mpm_diffuse_particle* staging;   // by particle id
     uint32_t* spawn_bits;            // by particle id
+    uint32_t* group_counts;          // spawners per group of kGroupIds ids
 };
 
 // Host record of a scene in a world.
@@ -140,6 +141,10 @@ struct World {
     int gbuf = 0;                           // i32 grid buffer the next substep accumulates into
     bool dens_valid = false;
     bool table_dirty = true;
+    // true when the last substep's G2P left every position's rank within its
+    // binning cell in rank/cell_count; adding or removing a scene clears it
+    // and the next substep recounts (k_count)
+    bool counted = false;
     uint64_t launches = 0;
     uint64_t generation = 1;                // bumps whenever the captured launch arguments change
 
