@@ -107,6 +107,7 @@ static void free_scene(Scene& s) {
         world_free(s.world);   // owns cmf/mvf of the binned engine
         s.cmf = nullptr;
         s.mvf = nullptr;
+        s.vel4 = nullptr;
     }
     void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
                     s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
@@ -304,6 +305,7 @@ mpm_status mpm_create(const mpm_desc* d, mpm_scene** out) {
     if (e == cudaSuccess && s.engine == kEngineBinned) {
         s.cmf = s.world.cmf;
         s.mvf = s.world.mvf;
+        s.vel4 = s.world.vel4;
     }
     if (e != cudaSuccess) {
         free_scene(s);

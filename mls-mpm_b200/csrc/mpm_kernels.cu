@@ -536,7 +536,9 @@ __global__ void __launch_bounds__(kGroupIds) k_spawn_write(const uint32_t* __res
 // slot; k_diffuse_kill_push then pushes killed slots in ascending slot order
 // (the order a one-at-a-time kill_particle, shaders.js:914-918, produces).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ f3 sample_grid_velocity(const float* __restrict__ mvf, const mpm_params& P, f3 pos) {
+// vel4 (binned engine): the same velocities as float4, one 16-byte load per cell.
+__device__ __forceinline__ f3 sample_grid_velocity(const float* __restrict__ mvf, const float4* __restrict__ vel4,
+                                                   const mpm_params& P, f3 pos) {
     const int32_t X = P.grid_X, Y = P.grid_Y, Z = P.grid_Z;
     int32_t cx, cy, cz;
     float fx, fy, fz;
@@ -560,9 +562,16 @@ __device__ __forceinline__ f3 sample_grid_velocity(const float* __restrict__ mvf
                 if (xx < 0 || xx >= X || yy < 0 || yy >= Y || zz < 0 || zz >= Z) continue;
                 const uint32_t idx = (uint32_t)((zz * Y + yy) * X + xx);
                 const float w = wx[i] * wy[j] * wz[k];
-                v.x += w * mvf[idx * 3u + 0u];
-                v.y += w * mvf[idx * 3u + 1u];
-                v.z += w * mvf[idx * 3u + 2u];
+                float cx, cy, cz;
+                if (vel4) {
+                    const float4 c = vel4[idx];
+                    cx = c.x; cy = c.y; cz = c.z;
+                } else {
+                    cx = mvf[idx * 3u + 0u]; cy = mvf[idx * 3u + 1u]; cz = mvf[idx * 3u + 2u];
+                }
+                v.x += w * cx;
+                v.y += w * cy;
+                v.z += w * cz;
             }
         }
     }
@@ -578,7 +587,8 @@ __device__ __forceinline__ void reflect_axis(float& p, float& v, float lo, float
 }
 
 __global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particle* __restrict__ pool,
-                                                              const float* __restrict__ mvf, const mpm_params P,
+                                                              const float* __restrict__ mvf,
+                                                              const float4* __restrict__ vel4, const mpm_params P,
                                                               const mpm_advect_params adv, const mpm_wall_params W,
                                                               uint32_t* __restrict__ kill_bits,
                                                               uint32_t* __restrict__ counts) {
@@ -595,13 +605,13 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particl
             p.pos[0] = pos3.x + dt * p.vel[0]; p.pos[1] = pos3.y + dt * p.vel[1]; p.pos[2] = pos3.z + dt * p.vel[2];
             p.pos[3] = 0.0f;
         } else if (p.ptype == MPM_DIFFUSE_FOAM) {
-            const f3 gv = sample_grid_velocity(mvf, P, pos3);
+            const f3 gv = sample_grid_velocity(mvf, vel4, P, pos3);
             p.pos[0] = pos3.x + dt * gv.x; p.pos[1] = pos3.y + dt * gv.y; p.pos[2] = pos3.z + dt * gv.z;
             p.pos[3] = 0.0f;
             p.lifetime -= dt;
             if (p.lifetime <= 0.0f) dead = true;
         } else if (p.ptype == MPM_DIFFUSE_BUBBLE) {
-            const f3 gv = sample_grid_velocity(mvf, P, pos3);
+            const f3 gv = sample_grid_velocity(mvf, vel4, P, pos3);
             p.vel[0] += dt * adv.drag * (gv.x - p.vel[0]);
             p.vel[1] += dt * (adv.buoyancy * -g + adv.drag * (gv.y - p.vel[1]));
             p.vel[2] += dt * adv.drag * (gv.z - p.vel[2]);
@@ -716,7 +726,8 @@ cudaError_t launch_diffuse(Scene& s, bool eval) {
     adv.diffuse_max = M;
     {
         Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
-        k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, P, adv, s.walls, d.kill_bits, d.block_counts);
+        k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, s.vel4, P, adv, s.walls, d.kill_bits,
+                                                  d.block_counts);
         k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mg, d.top, d.rank_state, 1);
         k_kill_push<<<mg, kGroupIds, 0, st>>>(d.kill_bits, M, d.block_counts, d.rank_state, d.free_list);
         s.launches += 3;

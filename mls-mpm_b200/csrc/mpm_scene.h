@@ -67,6 +67,7 @@ struct Scene {
     int32_t* mv = nullptr;
     float* cmf = nullptr;
     float* mvf = nullptr;
+    const float4* vel4 = nullptr;   // binned engine: the grid velocities as float4 (null: read mvf)
 
     DiffuseState diffuse;
     World world;              // binned engine: a world holding this one scene

@@ -745,7 +745,8 @@ __device__ __forceinline__ void hand_push(const mpm_hand_params& H, int32_t cx, 
 
 __global__ void __launch_bounds__(256) k_update_tiles(WorldView v, const int32_t* __restrict__ cm,
                                                       const int32_t* __restrict__ mv, float* __restrict__ mvf,
-                                                      int32_t* __restrict__ cm_next, int32_t* __restrict__ mv_next) {
+                                                      float4* __restrict__ vel4, int32_t* __restrict__ cm_next,
+                                                      int32_t* __restrict__ mv_next) {
     const uint32_t total = v.ctrl->n_grid * kTileCells;
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
         uint32_t idx;
@@ -763,6 +764,7 @@ __global__ void __launch_bounds__(256) k_update_tiles(WorldView v, const int32_t
             cz >= sd.hand_box[2] && cz <= sd.hand_box[5])
             hand_push(sd.H, cx, cy, cz, vx, vy, vz);
         out[0] = vx; out[1] = vy; out[2] = vz;
+        vel4[idx] = make_float4(vx, vy, vz, 0.0f);
     }
 }
 
@@ -1152,7 +1154,7 @@ struct G2PSum {
 
 // Returned by value: a pointer to the caller's accumulators would keep them
 // in local memory on the common (halo) path too.
-__device__ MPM_G2P_RARE G2PSum g2p_gather_direct(const PW w, const float4 q, const float* __restrict__ mvf,
+__device__ MPM_G2P_RARE G2PSum g2p_gather_direct(const PW w, const float4 q, const float4* __restrict__ vel4,
                                                  uint32_t X, uint32_t Y, uint32_t G) {
     G2PSum r;
     float& gvx = r.gv[0];
@@ -1177,8 +1179,8 @@ __device__ MPM_G2P_RARE G2PSum g2p_gather_direct(const PW w, const float4 q, con
                 const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)jj * X + (uint32_t)i;
                 float cvx = 0.0f, cvy = 0.0f, cvz = 0.0f;
                 if (cidx < G) {
-                    const float* c = mvf + 3ull * cidx;
-                    cvx = c[0]; cvy = c[1]; cvz = c[2];
+                    const float4 c = vel4[cidx];
+                    cvx = c.x; cvy = c.y; cvz = c.z;
                 }
                 const float wvx = ww * cvx, wvy = ww * cvy, wvz = ww * cvz;
                 gvx += wvx; gvy += wvy; gvz += wvz;
@@ -1243,16 +1245,16 @@ __device__ __forceinline__ void g2p_store(const G2POut& o, const SceneDesc& sd, 
 // G2P of a particle whose stencil leaves the halo box or the grid (rare): the
 // reference's linear stencil index with a bounds guard, then the epilogue.
 __device__ __noinline__ void g2p_direct_particle(const G2POut o, const SceneDesc* sdp, uint32_t p, const float4 q,
-                                                 const float4 vi, const float* __restrict__ mvf) {
+                                                 const float4 vi, const float4* __restrict__ vel4) {
     const SceneDesc& sd = *sdp;
     const PW w = particle_weights(q.x, q.y, q.z);
-    const G2PSum r = g2p_gather_direct(w, q, mvf, sd.X, sd.Y, sd.G);
+    const G2PSum r = g2p_gather_direct(w, q, vel4, sd.X, sd.Y, sd.G);
     g2p_store(o, sd, p, q, vi, r.gv[0], r.gv[1], r.gv[2], r.B);
 }
 
 __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(WorldView v, const float4* __restrict__ posm,
                                                               const float4* __restrict__ velid,
-                                                              const float* __restrict__ mvf,
+                                                              const float4* __restrict__ vel4,
                                                               const float* __restrict__ cmf,
                                                               float4* __restrict__ posm_out,
                                                               float4* __restrict__ velid_out,
@@ -1285,14 +1287,14 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         }
 #endif
         const int hn = halo_span(h);
-        const float* smvf = mvf + 3ull * sd.cell_base;
+        const float4* svel = vel4 + sd.cell_base;
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
             uint32_t cell;
             if (halo_cell(h, sd, i, cell)) {
-                const float* c = smvf + 3ull * cell;
-                vh[0][i] = c[0];
-                vh[1][i] = c[1];
-                vh[2][i] = c[2];
+                const float4 c = svel[cell];
+                vh[0][i] = c.x;
+                vh[1][i] = c.y;
+                vh[2][i] = c.z;
             } else {
                 vh[0][i] = 0.0f;
                 vh[1][i] = 0.0f;
@@ -1318,7 +1320,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
 #endif
             const PW w = particle_weights(q.x, q.y, q.z);
             if (!in_halo(w, h, sd)) {
-                g2p_direct_particle(out, &sd, p, q, vi, smvf);
+                g2p_direct_particle(out, &sd, p, q, vi, svel);
                 continue;
             }
             float gvx = 0.0f, gvy = 0.0f, gvz = 0.0f;
@@ -1407,6 +1409,7 @@ template <class F> static void world_arrays(World& w, F&& f) {
     f(w.ctrl, sizeof(Ctrl));
     f(w.cmf, C * 4);
     f(w.mvf, C * 12);
+    f(w.vel4, C * 16);
     f(w.d_scenes, (size_t)w.scene_cap * sizeof(SceneDesc));
 }
 
@@ -1451,6 +1454,7 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) e = cudaMemsetAsync(w.grid_i32[b], 0, C * 16, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.cmf, 0, C * 4, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.mvf, 0, C * 12, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.vel4, 0, C * 16, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.cell_count, 0, (C + 1) * 4, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.tile_flags, 0, T * 4, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.tile_occ, 0, T * 4, stream);
@@ -1618,6 +1622,7 @@ cudaError_t world_remove_scene(World& w, int slot) {
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(w.cmf + r.cell_base, 0, (size_t)r.G * 4, w.stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.mvf + 3ull * r.cell_base, 0, (size_t)r.G * 12, w.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.vel4 + r.cell_base, 0, (size_t)r.G * 16, w.stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.tile_flags + r.tile_base, 0, (size_t)r.ntiles * 4, w.stream);
     for (uint32_t t = 0; t < r.ntiles; ++t) w.h_tile_scene[r.tile_base + t] = kHole;
     if (e == cudaSuccess)
@@ -1713,7 +1718,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     }
     {
         Phase ph(prof, MPM_PHASE_UPDATE_GRID);   // includes APPLY_HAND
-        k_update_tiles<<<w.grid_blocks, 256, 0, st>>>(v, cm, mv, w.mvf, cm_n, mv_n);
+        k_update_tiles<<<w.grid_blocks, 256, 0, st>>>(v, cm, mv, w.mvf, w.vel4, cm_n, mv_n);
         w.launches++;
     }
     if (dv.enabled) {
@@ -1725,7 +1730,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     }
     {
         Phase ph(prof, MPM_PHASE_G2P);
-        k_g2p_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.mvf, w.cmf, w.posm[nxt],
+        k_g2p_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4, w.cmf, w.posm[nxt],
                                                             w.velid[nxt], w.aff[nxt], dv);
         w.launches++;
     }

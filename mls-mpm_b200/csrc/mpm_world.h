@@ -179,6 +179,7 @@ struct World {
     int32_t* cm_current = nullptr;               // buffer holding the last substep's P2G sums
     float* cmf = nullptr;                        // cells
     float* mvf = nullptr;                        // 3 cells
+    float4* vel4 = nullptr;                      // cells: (vx, vy, vz, 0), the same velocities 16-byte aligned
 
     // CUDA graphs of one substep (one per buffer parity), valid for `generation`
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
