@@ -516,6 +516,20 @@ __device__ __forceinline__ void chunk_header(const WorldView& v, uint32_t ch, Ch
     h.hz = z1 - z0 + 3;
 }
 
+// The chunk's scene descriptor in shared memory (copied when the scene
+// changes from the block's previous chunk), so per-particle reads of grid
+// dims and uniforms are shared-memory loads.  Block-uniform: every thread
+// calls it right after the chunk header is visible; `cached` is per thread.
+__device__ __forceinline__ void load_scene(const WorldView& v, uint32_t scene, SceneDesc& ssd, uint32_t& cached) {
+    static_assert(sizeof(SceneDesc) % 16 == 0, "SceneDesc copy in 16-byte words");
+    if (scene == cached) return;
+    const uint4* src = reinterpret_cast<const uint4*>(v.scenes + scene);
+    uint4* dst = reinterpret_cast<uint4*>(&ssd);
+    for (int i = threadIdx.x; i < (int)(sizeof(SceneDesc) / 16); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    cached = scene;
+}
+
 // True when the particle's 3x3x3 stencil lies in the chunk's halo box and in
 // the grid (then shared-memory accumulation / gathering is exact); otherwise
 // the particle takes the direct path with the reference's indexing.
@@ -589,10 +603,13 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     const uint32_t nch = v.ctrl->total_chunks;
     const uint32_t lane = threadIdx.x & 31;
     __shared__ ChunkHdr hs;
+    __shared__ SceneDesc ssd;
+    uint32_t cached = kHole;
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         if (threadIdx.x == 0) chunk_header(v, ch, hs);
         __syncthreads();
         const ChunkHdr h = hs;
+        load_scene(v, h.scene, ssd, cached);
         // this thread's particles, in flight while the halo is cleared
         float4 q[kPer];
 #pragma unroll
@@ -603,7 +620,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
         const int hn = halo_span(h);
         for (int i = threadIdx.x; i < hn; i += blockDim.x) acc[i] = 0;
         __syncthreads();
-        const SceneDesc& sd = v.scenes[h.scene];
+        const SceneDesc& sd = ssd;
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
             const bool valid = h.first + r * kChunkThreads + chunk_lane_offset() < h.end;
@@ -940,11 +957,14 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
     const uint32_t lane = threadIdx.x & 31;
     const size_t plane = v.npos;
     __shared__ ChunkHdr hs;
+    __shared__ SceneDesc ssd;
+    uint32_t cached = kHole;
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         if (threadIdx.x == 0) chunk_header(v, ch, hs);
         __syncthreads();
         const ChunkHdr h = hs;
-        const SceneDesc& sd = v.scenes[h.scene];
+        load_scene(v, h.scene, ssd, cached);
+        const SceneDesc& sd = ssd;
         const float* scmf = cmf + sd.cell_base;
         int32_t* smv = mv + 3ull * sd.cell_base;
         // the first particle's inputs are in flight while the halo is staged
@@ -1264,12 +1284,15 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     const uint32_t nch = v.ctrl->total_chunks;
     const size_t plane = v.npos;
     __shared__ ChunkHdr hs;
+    __shared__ SceneDesc ssd;
+    uint32_t cached = kHole;
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         // one thread reads the chunk header (measured faster here than every thread reading it)
         if (threadIdx.x == 0) chunk_header(v, ch, hs);
         __syncthreads();
         const ChunkHdr h = hs;
-        const SceneDesc& sd = v.scenes[h.scene];
+        load_scene(v, h.scene, ssd, cached);
+        const SceneDesc& sd = ssd;
 #if MPM_G2P_PREFETCH
         // this thread's particles, in flight while the halo is staged
         float4 qs[kPer], vis[kPer];
