@@ -940,9 +940,6 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
 #ifndef MPM_MOM_MINB
 #define MPM_MOM_MINB 2
 #endif
-#ifndef MPM_G2P_PREFETCH
-#define MPM_G2P_PREFETCH 0
-#endif
 
 __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(WorldView v, const float4* __restrict__ posm,
                                                                      const float4* __restrict__ velid,
@@ -1228,6 +1225,7 @@ struct G2POut {
     const float* dens;
     const float* cmf;                    // scene's decoded cell masses
     const mpm_gen_params* gen;           // null: no spawning for this scene
+    float bubble_min;                    // gen->density_bubble_min
     mpm_diffuse_particle* staging;
     uint32_t* spawn_bits;
     uint32_t* group_counts;
@@ -1235,9 +1233,12 @@ struct G2POut {
 
 // G2P epilogue of one particle (shaders.js:631-700): affine, advection and
 // boundary handling, the new state at position p, its binning key and tile
-// mark, and the diffuse spawn decision.
-__device__ __forceinline__ void g2p_store(const G2POut& o, const SceneDesc& sd, uint32_t p, const float4 q,
-                                          const float4 vi, float gvx, float gvy, float gvz, const float* B) {
+// mark, and the diffuse spawn decision.  Returns the particle's rank within
+// its new binning cell (the caller stores it at rank[p], as late as it can,
+// so the atomic's round trip overlaps later work).
+__device__ __forceinline__ uint32_t g2p_store(const G2POut& o, const SceneDesc& sd, uint32_t p, const float4 q,
+                                              const float4 vi, float density, float gvx, float gvy, float gvz,
+                                              const float* B) {
 #pragma unroll
     for (int e = 0; e < 9; ++e) o.aff[e * o.plane + p] = B[e] * 4.0f;
     f3 np, nv;
@@ -1250,16 +1251,22 @@ __device__ __forceinline__ void g2p_store(const G2POut& o, const SceneDesc& sd, 
     const uint32_t key = sd.cell_base + local_cell(sd, cx, cy, cz);
     o.key[p] = key;
     // the rank within the cell for the next substep's binning (k_count's work)
-    o.rank[p] = atomicAdd(&o.cell_count[key], 1u);
-    const uint32_t t = tile_of(sd, cx, cy, cz);
-    if ((o.tile_flags[t] & 1u) == 0u) atomicOr(&o.tile_flags[t], 1u);
+    const uint32_t rank = atomicAdd(&o.cell_count[key], 1u);
+    // occupied-tile mark: one fire-and-forget OR per distinct tile of the
+    // active lanes (consecutive positions mostly share one tile)
+    {
+        const uint32_t t = tile_of(sd, cx, cy, cz);
+        const unsigned act = __activemask();
+        const unsigned same = __match_any_sync(act, t);
+        if ((threadIdx.x & 31u) == (uint32_t)(__ffs(same) - 1)) atomicOr(&o.tile_flags[t], 1u);
+    }
     if (o.gen) {
         const uint32_t id = __float_as_uint(vi.w) - sd.id_base;
-        const float density = o.dens[p];
         // spawn_record's first test (shaders.js:806), checked inline
-        if (id < sd.n && density > 0.0f && density <= o.gen->density_bubble_min)
+        if (id < sd.n && density > 0.0f && density <= o.bubble_min)
             spawn_eval(id, np, nv, q.w, density, sd, o.cmf, o.gen, o.staging, o.spawn_bits, o.group_counts);
     }
+    return rank;
 }
 
 // G2P of a particle whose stencil leaves the halo box or the grid (rare): the
@@ -1269,7 +1276,7 @@ __device__ __noinline__ void g2p_direct_particle(const G2POut o, const SceneDesc
     const SceneDesc& sd = *sdp;
     const PW w = particle_weights(q.x, q.y, q.z);
     const G2PSum r = g2p_gather_direct(w, q, vel4, sd.X, sd.Y, sd.G);
-    g2p_store(o, sd, p, q, vi, r.gv[0], r.gv[1], r.gv[2], r.B);
+    o.rank[p] = g2p_store(o, sd, p, q, vi, o.dens[p], r.gv[0], r.gv[1], r.gv[2], r.B);
 }
 
 __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(WorldView v, const float4* __restrict__ posm,
@@ -1286,6 +1293,9 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     __shared__ ChunkHdr hs;
     __shared__ SceneDesc ssd;
     uint32_t cached = kHole;
+    // rank of the last particle whose atomic is still in flight
+    uint32_t pend_p = kHole, pend_rank = 0;
+    const float bubble_min = dv.enabled ? dv.gen->density_bubble_min : 0.0f;
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         // one thread reads the chunk header (measured faster here than every thread reading it)
         if (threadIdx.x == 0) chunk_header(v, ch, hs);
@@ -1293,22 +1303,22 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         const ChunkHdr h = hs;
         load_scene(v, h.scene, ssd, cached);
         const SceneDesc& sd = ssd;
-#if MPM_G2P_PREFETCH
         // this thread's particles, in flight while the halo is staged
-        float4 qs[kPer], vis[kPer];
+        float4 qs[kPer];
+        float ids[kPer], dns[kPer];
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
             const uint32_t p = h.first + r * kChunkThreads + threadIdx.x;
+            qs[r] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            ids[r] = 0.0f;
+            dns[r] = 0.0f;
             if (p < h.end) {
                 const uint32_t slot = v.perm[p];
                 qs[r] = posm[slot];
-                vis[r] = velid[slot];
-            } else {
-                qs[r] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                vis[r] = qs[r];
+                ids[r] = velid[slot].w;
+                dns[r] = v.dens[p];
             }
         }
-#endif
         const int hn = halo_span(h);
         const float4* svel = vel4 + sd.cell_base;
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
@@ -1327,20 +1337,14 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         __syncthreads();
         const bool spawn_scene = dv.enabled && h.scene == dv.scene;
         const G2POut out{posm_out, velid_out, aff_out, plane, v.key, v.rank, v.cell_count, v.tile_flags, v.dens,
-                         cmf + sd.cell_base,
-                         spawn_scene ? dv.gen : nullptr, dv.staging, dv.spawn_bits, dv.group_counts};
+                         cmf + sd.cell_base, spawn_scene ? dv.gen : nullptr, bubble_min, dv.staging, dv.spawn_bits,
+                         dv.group_counts};
 #pragma unroll 1
         for (int r = 0; r < kPer; ++r) {
             const uint32_t p = h.first + r * kChunkThreads + threadIdx.x;
             if (p >= h.end) break;
-#if MPM_G2P_PREFETCH
             const float4 q = qs[r];
-            const float4 vi = vis[r];
-#else
-            const uint32_t slot = v.perm[p];
-            const float4 q = posm[slot];
-            const float4 vi = velid[slot];
-#endif
+            const float4 vi = make_float4(0.0f, 0.0f, 0.0f, ids[r]);
             const PW w = particle_weights(q.x, q.y, q.z);
             if (!in_halo(w, h, sd)) {
                 g2p_direct_particle(out, &sd, p, q, vi, svel);
@@ -1373,10 +1377,15 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
                     }
                 }
             }
-            g2p_store(out, sd, p, q, vi, gvx, gvy, gvz, B);
+            const uint32_t rk = g2p_store(out, sd, p, q, vi, dns[r], gvx, gvy, gvz, B);
+            // the previous particle's rank: its atomic has long returned
+            if (pend_p != kHole) v.rank[pend_p] = pend_rank;
+            pend_p = p;
+            pend_rank = rk;
         }
         __syncthreads();
     }
+    if (pend_p != kHole) v.rank[pend_p] = pend_rank;
 }
 
 inline uint32_t cdiv(uint64_t a, uint32_t b) { return (uint32_t)((a + b - 1) / b); }
