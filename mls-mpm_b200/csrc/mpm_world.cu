@@ -95,7 +95,7 @@ WorldView World::view() const {
     v.tile_flags = tile_flags; v.tile_occ = tile_occ; v.tile_cnt = tile_cnt;
     v.tile_pstart = tile_pstart; v.tile_cstart = tile_cstart;
     v.group_pstart = group_pstart; v.group_cstart = group_cstart;
-    v.chunk_info = chunk_info; v.chunk_last = chunk_last;
+    v.chunk_info = chunk_info; v.chunk_last = chunk_last; v.chunk_hdr = chunk_hdr;
     v.tile_occ_list = tile_occ_list; v.tile_grid_list = tile_grid_list;
     v.ctrl = ctrl; v.dens = dens;
     return v;
@@ -516,6 +516,35 @@ __device__ __forceinline__ void chunk_header(const WorldView& v, uint32_t ch, Ch
     h.hz = z1 - z0 + 3;
 }
 
+// Asynchronous 16-byte global -> shared copy (cp.async); src_bytes 0 writes
+// zeros.  cp_async_wait waits for all of this thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, uint32_t src_bytes) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// ChunkHdr packed in two 16-byte words (box dims below 256).
+__device__ __forceinline__ void pack_header(const ChunkHdr& h, uint4* dst) {
+    dst[0] = make_uint4(h.scene, h.first, h.end, (uint32_t)h.hx | ((uint32_t)h.hy << 8) | ((uint32_t)h.hz << 16));
+    dst[1] = make_uint4((uint32_t)h.ox, (uint32_t)h.oy, (uint32_t)h.oz, 0u);
+}
+__device__ __forceinline__ ChunkHdr unpack_header(const uint4 a, const uint4 b) {
+    ChunkHdr h;
+    h.scene = a.x;
+    h.first = a.y;
+    h.end = a.z;
+    h.hx = (int32_t)(a.w & 0xFFu);
+    h.hy = (int32_t)((a.w >> 8) & 0xFFu);
+    h.hz = (int32_t)((a.w >> 16) & 0xFFu);
+    h.ox = (int32_t)b.x;
+    h.oy = (int32_t)b.y;
+    h.oz = (int32_t)b.z;
+    return h;
+}
+
 // The chunk's scene descriptor in shared memory (copied when the scene
 // changes from the block's previous chunk), so per-particle reads of grid
 // dims and uniforms are shared-memory loads.  Block-uniform: every thread
@@ -606,7 +635,10 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     __shared__ SceneDesc ssd;
     uint32_t cached = kHole;
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        if (threadIdx.x == 0) chunk_header(v, ch, hs);
+        if (threadIdx.x == 0) {
+            chunk_header(v, ch, hs);
+            pack_header(hs, v.chunk_hdr + 2ull * ch);   // for P2G_MOM and G2P
+        }
         __syncthreads();
         const ChunkHdr h = hs;
         load_scene(v, h.scene, ssd, cached);
@@ -956,10 +988,17 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
     __shared__ ChunkHdr hs;
     __shared__ SceneDesc ssd;
     uint32_t cached = kHole;
+    // chunk headers: the next one's words are loaded while this chunk runs
+    uint4 nh0 = make_uint4(0u, 0u, 0u, 0u), nh1 = nh0;
+    if (threadIdx.x == 0 && blockIdx.x < nch) hs = unpack_header(v.chunk_hdr[2ull * blockIdx.x], v.chunk_hdr[2ull * blockIdx.x + 1]);
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        if (threadIdx.x == 0) chunk_header(v, ch, hs);
         __syncthreads();
         const ChunkHdr h = hs;
+        const uint32_t nxt = ch + gridDim.x;
+        if (threadIdx.x == 0 && nxt < nch) {
+            nh0 = v.chunk_hdr[2ull * nxt];
+            nh1 = v.chunk_hdr[2ull * nxt + 1];
+        }
         load_scene(v, h.scene, ssd, cached);
         const SceneDesc& sd = ssd;
         const float* scmf = cmf + sd.cell_base;
@@ -979,12 +1018,26 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
             for (int e = 0; e < 9; ++e) a[e] = valid ? aff[e * plane + slot] : 0.0f;
         }
         const int hn = halo_span(h);
-        for (int i = threadIdx.x; i < hn; i += blockDim.x) {
-            uint32_t cell;
-            mh[i] = halo_cell(h, sd, i, cell) ? scmf[cell] : 0.0f;
-            acc[0][i] = 0;
-            acc[1][i] = 0;
-            acc[2][i] = 0;
+        {
+            // every load of the staging in flight before the first store
+            constexpr int kIt = (kHaloCells + kChunkThreads - 1) / kChunkThreads;
+            float m[kIt];
+#pragma unroll
+            for (int it = 0; it < kIt; ++it) {
+                const int i = threadIdx.x + it * kChunkThreads;
+                uint32_t cell;
+                m[it] = (i < hn && halo_cell(h, sd, i, cell)) ? scmf[cell] : 0.0f;
+            }
+#pragma unroll
+            for (int it = 0; it < kIt; ++it) {
+                const int i = threadIdx.x + it * kChunkThreads;
+                if (i < hn) {
+                    mh[i] = m[it];
+                    acc[0][i] = 0;
+                    acc[1][i] = 0;
+                    acc[2][i] = 0;
+                }
+            }
         }
         __syncthreads();
 #pragma unroll 1
@@ -1036,6 +1089,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
             }
         }
         __syncthreads();
+        if (threadIdx.x == 0 && nxt < nch) hs = unpack_header(nh0, nh1);
     }
 }
 
@@ -1287,7 +1341,8 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
                                                               float4* __restrict__ velid_out,
                                                               float* __restrict__ aff_out, DiffuseView dv) {
     constexpr int kPer = kChunk / kChunkThreads;
-    __shared__ float vh[3][kHaloCells];
+    __shared__ float4 vh[kHaloCells];   // staged grid velocities (x, y, z, 0)
+    __shared__ uint4 nhs[2];              // the next chunk's header words
     const uint32_t nch = v.ctrl->total_chunks;
     const size_t plane = v.npos;
     __shared__ ChunkHdr hs;
@@ -1296,11 +1351,16 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     // rank of the last particle whose atomic is still in flight
     uint32_t pend_p = kHole, pend_rank = 0;
     const float bubble_min = dv.enabled ? dv.gen->density_bubble_min : 0.0f;
+    // chunk headers: the next one's words are copied while this chunk runs
+    if (threadIdx.x == 0 && blockIdx.x < nch) hs = unpack_header(v.chunk_hdr[2ull * blockIdx.x], v.chunk_hdr[2ull * blockIdx.x + 1]);
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        // one thread reads the chunk header (measured faster here than every thread reading it)
-        if (threadIdx.x == 0) chunk_header(v, ch, hs);
         __syncthreads();
         const ChunkHdr h = hs;
+        const uint32_t nxt = ch + gridDim.x;
+        if (threadIdx.x == 0 && nxt < nch) {
+            cp_async16(&nhs[0], v.chunk_hdr + 2ull * nxt, 16u);
+            cp_async16(&nhs[1], v.chunk_hdr + 2ull * nxt + 1, 16u);
+        }
         load_scene(v, h.scene, ssd, cached);
         const SceneDesc& sd = ssd;
         // this thread's particles, in flight while the halo is staged
@@ -1323,17 +1383,10 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         const float4* svel = vel4 + sd.cell_base;
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
             uint32_t cell;
-            if (halo_cell(h, sd, i, cell)) {
-                const float4 c = svel[cell];
-                vh[0][i] = c.x;
-                vh[1][i] = c.y;
-                vh[2][i] = c.z;
-            } else {
-                vh[0][i] = 0.0f;
-                vh[1][i] = 0.0f;
-                vh[2][i] = 0.0f;
-            }
+            const bool in = halo_cell(h, sd, i, cell);
+            cp_async16(&vh[i], in ? (const void*)(svel + cell) : (const void*)svel, in ? 16u : 0u);
         }
+        cp_async_wait();
         __syncthreads();
         const bool spawn_scene = dv.enabled && h.scene == dv.scene;
         const G2POut out{posm_out, velid_out, aff_out, plane, v.key, v.rank, v.cell_count, v.tile_flags, v.dens,
@@ -1367,8 +1420,8 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
                         for (int i = 0; i < 3; ++i) {
                             const float ww = w.wx[i] * wyzk;
                             const float dxi = __int2float_rn(bx + i) - q.x + 0.5f;
-                            const int hi = hb + k * kHXY + jj * kHX + i;
-                            const float wvx = ww * vh[0][hi], wvy = ww * vh[1][hi], wvz = ww * vh[2][hi];
+                            const float4 c = vh[hb + k * kHXY + jj * kHX + i];
+                            const float wvx = ww * c.x, wvy = ww * c.y, wvz = ww * c.z;
                             gvx += wvx; gvy += wvy; gvz += wvz;
                             B[0] += wvx * dxi; B[1] += wvx * dyj; B[2] += wvx * dzk;
                             B[3] += wvy * dxi; B[4] += wvy * dyj; B[5] += wvy * dzk;
@@ -1384,6 +1437,10 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
             pend_rank = rk;
         }
         __syncthreads();
+        if (threadIdx.x == 0 && nxt < nch) {
+            cp_async_wait();
+            hs = unpack_header(nhs[0], nhs[1]);
+        }
     }
     if (pend_p != kHole) v.rank[pend_p] = pend_rank;
 }
@@ -1435,6 +1492,7 @@ template <class F> static void world_arrays(World& w, F&& f) {
     f(w.group_cstart, NG * 4);
     f(w.chunk_info, (size_t)w.chunk_cap * 16);
     f(w.chunk_last, (size_t)w.chunk_cap * 4);
+    f(w.chunk_hdr, (size_t)w.chunk_cap * 32);
     f(w.tile_occ_list, T * 4);
     f(w.tile_grid_list, T * 4);
     f(w.tile_scene, T * 4);

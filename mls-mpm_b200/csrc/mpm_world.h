@@ -87,6 +87,7 @@ struct WorldView {
     uint32_t* group_cstart;    // per group: exclusive scan of the group chunk totals
     uint4* chunk_info;         // per chunk: (tile, first position, end position, first local cell)
     uint32_t* chunk_last;      // per chunk: last local cell
+    uint4* chunk_hdr;          // per chunk, 2 words: the packed ChunkHdr (written by P2G_MASS)
     uint32_t* tile_occ_list;
     uint32_t* tile_grid_list;
     Ctrl* ctrl;
@@ -171,6 +172,7 @@ struct World {
     uint32_t* group_cstart = nullptr;
     uint4* chunk_info = nullptr;
     uint32_t* chunk_last = nullptr;
+    uint4* chunk_hdr = nullptr;
     uint32_t chunk_cap = 0;
     uint32_t* tile_occ_list = nullptr;
     uint32_t* tile_grid_list = nullptr;
