@@ -1125,20 +1125,42 @@ __device__ __forceinline__ bool estimate_normal_f(const float* __restrict__ cmf,
 #else
 #define MPM_G2P_RARE __noinline__
 #endif
-__device__ MPM_G2P_RARE void spawn_eval(uint32_t id, f3 np, f3 nv, float m, float density, const SceneDesc& sd,
-                                        const float* __restrict__ cmf, const mpm_gen_params* __restrict__ genp,
-                                        mpm_diffuse_particle* __restrict__ staging,
-                                        uint32_t* __restrict__ spawn_bits, uint32_t* __restrict__ group_counts) {
-    const mpm_gen_params& gen = *genp;
-    const f3 vel = nv;
+// The spawn test's terms that need no neighbour data (shaders.js:807-815):
+// speed, kinetic energy and trapped air.
+struct SpawnPre {
+    float speed, ke, trappedAir;
+};
+
+__device__ __forceinline__ SpawnPre spawn_pre(f3 vel, float m, float density, const SceneDesc& sd,
+                                              float pressure_threshold) {
+    SpawnPre r;
     const float speed2 = dot3(vel, vel);
-    const float speed = __fsqrt_rn(speed2);
-    const float ke = 0.5f * m * speed2;
+    r.speed = __fsqrt_rn(speed2);
+    r.ke = 0.5f * m * speed2;
     const float rest = sd.P.rest_density;
     float pressure = sd.P.stiffness * (eos_pow(__fdiv_rn(density, rest), sd.P.eos_power) - 1.0f);
     const float pFloor = density > rest * kCohesionGate ? kCohesionPressure : 0.0f;
     pressure = fmaxf(pressure, pFloor);
-    const float trappedAir = fmaxf(0.0f, pressure - gen.pressure_threshold);
+    r.trappedAir = fmaxf(0.0f, pressure - pressure_threshold);
+    return r;
+}
+
+// True when the score cannot reach ke_threshold whatever the wave-crest term:
+// that term is dotVal * speed with dotVal the dot product of two unit vectors
+// (below 1.0001 after rounding), and every operation is rounded monotonically,
+// so the score evaluated with 1.0001 * speed in its place bounds the real one.
+__device__ __forceinline__ bool spawn_hopeless(const SpawnPre& s, float ke_threshold) {
+    return (s.ke + s.trappedAir * 2.0f) + (1.0001f * s.speed) * 1.5f < ke_threshold;
+}
+
+__device__ MPM_G2P_RARE void spawn_eval(uint32_t id, f3 np, f3 nv, float density, SpawnPre pre,
+                                        const SceneDesc& sd, const float* __restrict__ cmf,
+                                        const mpm_gen_params* __restrict__ genp,
+                                        mpm_diffuse_particle* __restrict__ staging,
+                                        uint32_t* __restrict__ spawn_bits, uint32_t* __restrict__ group_counts) {
+    const mpm_gen_params& gen = *genp;
+    const f3 vel = nv;
+    const float speed = pre.speed, ke = pre.ke, trappedAir = pre.trappedAir;
     f3 nrm;
     const bool ok = estimate_normal_f(cmf, sd, np.x, np.y, np.z, nrm);
     float waveCrest = 0.0f;
@@ -1280,6 +1302,8 @@ struct G2POut {
     const float* cmf;                    // scene's decoded cell masses
     const mpm_gen_params* gen;           // null: no spawning for this scene
     float bubble_min;                    // gen->density_bubble_min
+    float pressure_threshold;            // gen->pressure_threshold
+    float ke_threshold;                  // gen->ke_threshold
     mpm_diffuse_particle* staging;
     uint32_t* spawn_bits;
     uint32_t* group_counts;
@@ -1317,8 +1341,11 @@ __device__ __forceinline__ uint32_t g2p_store(const G2POut& o, const SceneDesc& 
     if (o.gen) {
         const uint32_t id = __float_as_uint(vi.w) - sd.id_base;
         // spawn_record's first test (shaders.js:806), checked inline
-        if (id < sd.n && density > 0.0f && density <= o.bubble_min)
-            spawn_eval(id, np, nv, q.w, density, sd, o.cmf, o.gen, o.staging, o.spawn_bits, o.group_counts);
+        if (id < sd.n && density > 0.0f && density <= o.bubble_min) {
+            const SpawnPre pre = spawn_pre(nv, q.w, density, sd, o.pressure_threshold);
+            if (!spawn_hopeless(pre, o.ke_threshold))
+                spawn_eval(id, np, nv, density, pre, sd, o.cmf, o.gen, o.staging, o.spawn_bits, o.group_counts);
+        }
     }
     return rank;
 }
@@ -1351,6 +1378,8 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     // rank of the last particle whose atomic is still in flight
     uint32_t pend_p = kHole, pend_rank = 0;
     const float bubble_min = dv.enabled ? dv.gen->density_bubble_min : 0.0f;
+    const float pressure_threshold = dv.enabled ? dv.gen->pressure_threshold : 0.0f;
+    const float ke_threshold = dv.enabled ? dv.gen->ke_threshold : 0.0f;
     // chunk headers: the next one's words are copied while this chunk runs
     if (threadIdx.x == 0 && blockIdx.x < nch) hs = unpack_header(v.chunk_hdr[2ull * blockIdx.x], v.chunk_hdr[2ull * blockIdx.x + 1]);
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
@@ -1390,8 +1419,8 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         __syncthreads();
         const bool spawn_scene = dv.enabled && h.scene == dv.scene;
         const G2POut out{posm_out, velid_out, aff_out, plane, v.key, v.rank, v.cell_count, v.tile_flags, v.dens,
-                         cmf + sd.cell_base, spawn_scene ? dv.gen : nullptr, bubble_min, dv.staging, dv.spawn_bits,
-                         dv.group_counts};
+                         cmf + sd.cell_base, spawn_scene ? dv.gen : nullptr, bubble_min, pressure_threshold,
+                         ke_threshold, dv.staging, dv.spawn_bits, dv.group_counts};
 #pragma unroll 1
         for (int r = 0; r < kPer; ++r) {
             const uint32_t p = h.first + r * kChunkThreads + threadIdx.x;
