@@ -112,7 +112,8 @@ static void free_scene(Scene& s) {
     void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
                     s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
                     s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.rank_state, s.diffuse.staging,
-                    s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word, s.diffuse.gen_dev};
+                    s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word, s.diffuse.gen_dev,
+                    s.diffuse.adv_dev};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s.diffuse.host_top) cudaFreeHost(s.diffuse.host_top);
@@ -427,6 +428,7 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     if (e == cudaSuccess) e = dalloc(&d.rank_state, 16);
     if (e == cudaSuccess) e = dalloc(&d.staging, N * 48);
     if (e == cudaSuccess) e = dalloc(&d.gen_dev, sizeof(mpm_gen_params));
+    if (e == cudaSuccess) e = dalloc(&d.adv_dev, sizeof(mpm_advect_params));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&d.host_top, 16);
     if (e != cudaSuccess) return cuda_fail(e, "mpm_diffuse_enable allocation");
     // diffuse-gpu.js:60-68: free list [0..M-1], top = M, all slots dead
@@ -444,6 +446,8 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     d.seed = gen->seed;
     CUDA_TRY(cudaMemcpyAsync(d.gen_dev, &d.gen, sizeof(mpm_gen_params), cudaMemcpyHostToDevice, s.stream),
              "gen params");
+    CUDA_TRY(cudaMemcpyAsync(d.adv_dev, &d.adv, sizeof(mpm_advect_params), cudaMemcpyHostToDevice, s.stream),
+             "advect params");
     d.enabled = true;
     return MPM_OK;
 }

@@ -586,12 +586,10 @@ __device__ __forceinline__ void reflect_axis(float& p, float& v, float lo, float
     v = nv;
 }
 
-__global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particle* __restrict__ pool,
-                                                              const float* __restrict__ mvf,
-                                                              const float4* __restrict__ vel4, const mpm_params P,
-                                                              const mpm_advect_params adv, const mpm_wall_params W,
-                                                              uint32_t* __restrict__ kill_bits,
-                                                              uint32_t* __restrict__ counts) {
+__device__ __forceinline__ void diffuse_advect(mpm_diffuse_particle* __restrict__ pool, const float* __restrict__ mvf,
+                                               const float4* __restrict__ vel4, const mpm_params& P,
+                                               const mpm_advect_params& adv, const mpm_wall_params& W,
+                                               uint32_t* __restrict__ kill_bits, uint32_t* __restrict__ counts) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t M = adv.diffuse_max;
     bool kill = false;
@@ -667,6 +665,27 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particl
     }
 }
 
+// ADVECT with the uniforms as kernel parameters (plain engine).
+__global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particle* __restrict__ pool,
+                                                              const float* __restrict__ mvf,
+                                                              const float4* __restrict__ vel4, const mpm_params P,
+                                                              const mpm_advect_params adv, const mpm_wall_params W,
+                                                              uint32_t* __restrict__ kill_bits,
+                                                              uint32_t* __restrict__ counts) {
+    diffuse_advect(pool, mvf, vel4, P, adv, W, kill_bits, counts);
+}
+
+// ADVECT with the uniforms read from device memory (binned engine; graph-capturable).
+__global__ void __launch_bounds__(kThreads) k_diffuse_advect_dev(mpm_diffuse_particle* __restrict__ pool,
+                                                                  const float4* __restrict__ vel4,
+                                                                  const mpm_params* __restrict__ P,
+                                                                  const mpm_advect_params* __restrict__ adv,
+                                                                  const mpm_wall_params* __restrict__ W,
+                                                                  uint32_t* __restrict__ kill_bits,
+                                                                  uint32_t* __restrict__ counts) {
+    diffuse_advect(pool, nullptr, vel4, *P, *adv, *W, kill_bits, counts);
+}
+
 // Killed slots in ascending order go to free_list[top], free_list[top+1], ...
 // One block per group of kGroupIds slots (counts: exclusive group offsets,
 // state[1] the total); groups without kills return at once.
@@ -694,7 +713,7 @@ cudaError_t launch_apply_hand(Scene& s) {
 // DiffuseGPU.step (diffuse-gpu.js:148-166) after G2P.  With eval the spawn
 // decision pass runs here (plain engine); the binned engine makes that
 // decision in its G2P epilogue and has already bumped the seed.
-cudaError_t launch_diffuse(Scene& s, bool eval) {
+cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const mpm_wall_params* W_dev) {
     static_assert(kThreads == (int)kGroupIds, "one rank group per 256-thread block");
     cudaStream_t st = s.stream;
     const mpm_params& P = s.params;
@@ -726,8 +745,12 @@ cudaError_t launch_diffuse(Scene& s, bool eval) {
     adv.diffuse_max = M;
     {
         Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
-        k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, s.vel4, P, adv, s.walls, d.kill_bits,
-                                                  d.block_counts);
+        if (P_dev && W_dev && s.vel4)
+            k_diffuse_advect_dev<<<mg, kThreads, 0, st>>>(d.pool, s.vel4, P_dev, d.adv_dev, W_dev, d.kill_bits,
+                                                          d.block_counts);
+        else
+            k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, s.vel4, P, adv, s.walls, d.kill_bits,
+                                                      d.block_counts);
         k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mg, d.top, d.rank_state, 1);
         k_kill_push<<<mg, kGroupIds, 0, st>>>(d.kill_bits, M, d.block_counts, d.rank_state, d.free_list);
         s.launches += 3;

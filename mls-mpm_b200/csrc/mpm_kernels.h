@@ -14,6 +14,10 @@ cudaError_t launch_substep_plain(Scene& s);
 cudaError_t launch_apply_hand(Scene& s);
 
 // DiffuseGPU.step after G2P; eval = run the spawn-decision pass here.
-cudaError_t launch_diffuse(Scene& s, bool eval);
+// P_dev / W_dev (binned engine): the scene's uniforms in device memory, read
+// by ADVECT instead of the host copies, so the launches can be captured in a
+// CUDA graph and replayed with uniforms uploaded later.
+cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev = nullptr,
+                           const mpm_wall_params* W_dev = nullptr);
 
 }  // namespace mpm

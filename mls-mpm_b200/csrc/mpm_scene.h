@@ -34,6 +34,7 @@ struct DiffuseState {
     mpm_diffuse_particle* staging = nullptr;  // N x 48 B spawn records indexed by particle id
     int32_t* host_top = nullptr;            // pinned 4 B for alive-count readback
     mpm_gen_params* gen_dev = nullptr;      // device GenParams (binned engine: seed bumped on the device)
+    mpm_advect_params* adv_dev = nullptr;   // device copy of adv (binned engine)
 };
 
 // Engines: the binned item-major substep (default) and the plain per-pass

@@ -1863,7 +1863,8 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     if (e != cudaSuccess) return e;
     if (dv.enabled) {
         ds->diffuse.seed += 1u;   // mirrors the device-side bump in k_tile_scan_top
-        e = launch_diffuse(*ds, false);
+        const SceneDesc* sd_dev = w.d_scenes + dv.scene;
+        e = launch_diffuse(*ds, false, &sd_dev->P, &sd_dev->W);
     }
     return e;
 }
@@ -1874,9 +1875,12 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
     const bool diffuse = ds && ds->diffuse.enabled;
     const bool profiling = ds && ds->profile;
     // a substep that must recount runs eagerly; the captured graphs never count
-    if (!use_graph || diffuse || profiling || !w.counted) return enqueue_substep(w, ds);
+    if (!use_graph || profiling || !w.counted) return enqueue_substep(w, ds);
+    // the diffuse update joins the graph: its kernels read the uniforms from
+    // the device scene table and the advect parameters from a device copy
+    Scene* dsc = diffuse ? ds : nullptr;
     const int p = w.cur;   // cur and gbuf flip together: one graph per parity
-    if (!w.graph[p] || w.graph_gen[p] != w.generation) {
+    if (!w.graph[p] || w.graph_gen[p] != w.generation || w.graph_diffuse[p] != diffuse) {
         if (w.graph[p]) {
             cudaGraphExecDestroy(w.graph[p]);
             w.graph[p] = nullptr;
@@ -1885,31 +1889,39 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
         int32_t* cmc0 = w.cm_current;
         const bool dv0 = w.dens_valid;
         const uint64_t l0 = w.launches;
+        const uint64_t sl0 = dsc ? dsc->launches : 0;
+        const uint32_t seed0 = dsc ? dsc->diffuse.seed : 0;
         cudaGraph_t g = nullptr;
         e = cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;
-        const cudaError_t e2 = enqueue_substep(w, nullptr);
+        const cudaError_t e2 = enqueue_substep(w, dsc);
         e = cudaStreamEndCapture(w.stream, &g);
         if (e2 != cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaGraphInstantiate(&w.graph[p], g, 0);
         if (g) cudaGraphDestroy(g);
         // capture only recorded the work: restore the host state the enqueue advanced
-        w.graph_kernels[p] = w.launches - l0;
+        w.graph_kernels[p] = w.launches - l0 + (dsc ? dsc->launches - sl0 : 0);
         w.cur = cur0;
         w.gbuf = gbuf0;
         w.cm_current = cmc0;
         w.dens_valid = dv0;
         w.launches = l0;
+        if (dsc) {
+            dsc->launches = sl0;
+            dsc->diffuse.seed = seed0;
+        }
         if (e != cudaSuccess) {
             w.graph[p] = nullptr;
             return e;
         }
         w.graph_gen[p] = w.generation;
+        w.graph_diffuse[p] = diffuse;
     }
     e = cudaGraphLaunch(w.graph[p], w.stream);
     if (e != cudaSuccess) return e;
     // host mirror of what the graph does
     w.launches += w.graph_kernels[p];
+    if (dsc) dsc->diffuse.seed += 1u;
     w.pos_bound = w.n_total;   // the layout after a substep is dense
     w.cm_current = w.grid_i32[w.gbuf];
     w.cur ^= 1;

@@ -187,6 +187,7 @@ struct World {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_gen[2] = {0, 0};
     uint64_t graph_kernels[2] = {0, 0};     // kernels in each graph (launch accounting)
+    bool graph_diffuse[2] = {false, false};  // the graph includes the diffuse update of its scene
 
     WorldView view() const;
 };
