@@ -95,7 +95,7 @@ WorldView World::view() const {
     v.tile_flags = tile_flags; v.tile_occ = tile_occ; v.tile_cnt = tile_cnt;
     v.tile_pstart = tile_pstart; v.tile_cstart = tile_cstart;
     v.group_pstart = group_pstart; v.group_cstart = group_cstart;
-    v.chunk_info = chunk_info; v.chunk_last = chunk_last; v.chunk_hdr = chunk_hdr;
+    v.chunk_info = chunk_info; v.chunk_last = chunk_last; v.chunk_hdr = chunk_hdr; v.chunk_geo = chunk_geo;
     v.tile_occ_list = tile_occ_list; v.tile_grid_list = tile_grid_list;
     v.ctrl = ctrl; v.dens = dens;
     return v;
@@ -411,7 +411,10 @@ __global__ void __launch_bounds__(kTileCells) k_tile_finish(WorldView v) {
             if (ci >= v.chunk_cap) break;
             const uint32_t f = j * kChunk;
             const uint32_t e = min(f + kChunk, total);
-            if (f >= a) v.chunk_info[ci] = make_uint4(t, base_p + f, base_p + e, lid);
+            if (f >= a) {
+                v.chunk_info[ci] = make_uint4(t, base_p + f, base_p + e, lid);
+                v.chunk_geo[ci] = make_uint4(scene, tx, ty, tz);
+            }
             if (e - 1 < a + cnt) v.chunk_last[ci] = lid;
         }
     }
@@ -485,15 +488,12 @@ struct ChunkHdr {
 
 // The box of the local cells [lo, hi] (x fastest, then y, then z) plus one
 // cell on every side.
-__device__ __forceinline__ void chunk_header(const WorldView& v, uint32_t ch, ChunkHdr& h) {
-    const uint4 ci = v.chunk_info[ch];
-    const uint32_t lo = ci.w, hi = v.chunk_last[ch];
-    const uint32_t t = ci.x;
-    const uint32_t scene = v.tile_scene[t];
-    const SceneDesc& sd = v.scenes[scene];
-    const uint32_t lt = t - sd.tile_base;
-    const int32_t tx = (int32_t)(lt % sd.ntx), ty = (int32_t)((lt / sd.ntx) % sd.nty),
-                  tz = (int32_t)(lt / (sd.ntx * sd.nty));
+// The chunk's header from its three independent words: chunk_info (tile,
+// first, end, first local cell), chunk_last (last local cell) and chunk_geo
+// (scene, tile coordinates).
+__device__ __forceinline__ void chunk_header_from(const uint4 ci, uint32_t hi, const uint4 geo, ChunkHdr& h) {
+    const uint32_t lo = ci.w;
+    const int32_t tx = (int32_t)geo.y, ty = (int32_t)geo.z, tz = (int32_t)geo.w;
     constexpr uint32_t kRow = kTileX, kSlab = kTileX * kTileY;
     int32_t x0 = 0, x1 = kTileX - 1, y0 = 0, y1 = kTileY - 1;
     const int32_t z0 = (int32_t)(lo / kSlab), z1 = (int32_t)(hi / kSlab);
@@ -505,7 +505,7 @@ __device__ __forceinline__ void chunk_header(const WorldView& v, uint32_t ch, Ch
             x1 = (int32_t)(hi % kRow);
         }
     }
-    h.scene = scene;
+    h.scene = geo.x;
     h.first = ci.y;
     h.end = ci.z;
     h.ox = tx * kTileX + x0 - 1;
@@ -634,13 +634,23 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     __shared__ ChunkHdr hs;
     __shared__ SceneDesc ssd;
     uint32_t cached = kHole;
+    // thread 0: the next chunk's header words, loaded while this chunk runs
+    uint4 nci = make_uint4(0u, 0u, 0u, 0u), ngeo = nci;
+    uint32_t nlast = 0;
+    if (threadIdx.x == 0 && blockIdx.x < nch)
+        chunk_header_from(v.chunk_info[blockIdx.x], v.chunk_last[blockIdx.x], v.chunk_geo[blockIdx.x], hs);
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        if (threadIdx.x == 0) {
-            chunk_header(v, ch, hs);
-            pack_header(hs, v.chunk_hdr + 2ull * ch);   // for P2G_MOM and G2P
-        }
         __syncthreads();
         const ChunkHdr h = hs;
+        const uint32_t nxt = ch + gridDim.x;
+        if (threadIdx.x == 0) {
+            pack_header(h, v.chunk_hdr + 2ull * ch);   // for P2G_MOM and G2P
+            if (nxt < nch) {
+                nci = v.chunk_info[nxt];
+                nlast = v.chunk_last[nxt];
+                ngeo = v.chunk_geo[nxt];
+            }
+        }
         load_scene(v, h.scene, ssd, cached);
         // this thread's particles, in flight while the halo is cleared
         float4 q[kPer];
@@ -696,6 +706,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             if (a != 0 && halo_cell(h, sd, i, cell)) atomicAdd(&scm[cell], a);
         }
         __syncthreads();
+        if (threadIdx.x == 0 && nxt < nch) chunk_header_from(nci, nlast, ngeo, hs);
     }
 }
 
@@ -1522,6 +1533,7 @@ template <class F> static void world_arrays(World& w, F&& f) {
     f(w.chunk_info, (size_t)w.chunk_cap * 16);
     f(w.chunk_last, (size_t)w.chunk_cap * 4);
     f(w.chunk_hdr, (size_t)w.chunk_cap * 32);
+    f(w.chunk_geo, (size_t)w.chunk_cap * 16);
     f(w.tile_occ_list, T * 4);
     f(w.tile_grid_list, T * 4);
     f(w.tile_scene, T * 4);

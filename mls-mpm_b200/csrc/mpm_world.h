@@ -88,6 +88,7 @@ struct WorldView {
     uint4* chunk_info;         // per chunk: (tile, first position, end position, first local cell)
     uint32_t* chunk_last;      // per chunk: last local cell
     uint4* chunk_hdr;          // per chunk, 2 words: the packed ChunkHdr (written by P2G_MASS)
+    uint4* chunk_geo;          // per chunk: (scene, tile x, tile y, tile z) of its tile
     uint32_t* tile_occ_list;
     uint32_t* tile_grid_list;
     Ctrl* ctrl;
@@ -173,6 +174,7 @@ struct World {
     uint4* chunk_info = nullptr;
     uint32_t* chunk_last = nullptr;
     uint4* chunk_hdr = nullptr;
+    uint4* chunk_geo = nullptr;
     uint32_t chunk_cap = 0;
     uint32_t* tile_occ_list = nullptr;
     uint32_t* tile_grid_list = nullptr;
