@@ -890,6 +890,84 @@ __device__ __forceinline__ void mom_contrib(const PW& w, const MomIn& in, const 
     }
 }
 
+// The shared-halo form of mom_contrib with every loop written out at compile
+// time (template indices): the 81 contributions go straight into the three
+// accumulator arrays at base slot hb with immediate offsets.
+struct MomTerms {
+    float dxs[3], dys[3];
+    float qz[3][3], fz[3][3];   // [component][k]
+    float s00, s11, s01, s02, s12;
+    float coef;
+};
+
+template <bool kClamp, int K, int J, int I>
+__device__ __forceinline__ void mom_cell(const PW& w, const MomIn& in, const MomTerms& t, float qx, float qy,
+                                         float qzz, float gx, float gy, float gz, int32_t* a0, int32_t* a1,
+                                         int32_t* a2) {
+    const float ww = w.wx[I] * (w.wy[J] * w.wz[K]);
+    const float Qx = qx + t.qz[0][K];
+    const float Qy = qy + t.qz[1][K];
+    const float Qz = qzz + t.qz[2][K];
+    const float fxf = t.coef * (gx + t.fz[0][K]);
+    const float fyf = t.coef * (gy + t.fz[1][K]);
+    const float fzf = t.coef * (gz + t.fz[2][K]);
+    const float vx = ww * (in.m * (in.vx + Qx) + fxf);
+    const float vy = ww * (in.m * (in.vy + Qy) + fyf);
+    const float vz = ww * (in.m * (in.vz + Qz) + fzf);
+    constexpr int o = K * kHXY + J * kHX + I;
+    atomicAdd(a0 + o, kClamp ? encode(vx) : encode_unclamped(vx));
+    atomicAdd(a1 + o, kClamp ? encode(vy) : encode_unclamped(vy));
+    atomicAdd(a2 + o, kClamp ? encode(vz) : encode_unclamped(vz));
+}
+
+template <bool kClamp, int J, int I>
+__device__ __forceinline__ void mom_column(const PW& w, const MomIn& in, const MomTerms& t, int32_t* a0,
+                                           int32_t* a1, int32_t* a2) {
+    const float dxi = t.dxs[I], dyj = t.dys[J];
+    const float qx = in.a00 * dxi + in.a01 * dyj;
+    const float qy = in.a10 * dxi + in.a11 * dyj;
+    const float qzz = in.a20 * dxi + in.a21 * dyj;
+    const float gx = t.s00 * dxi + t.s01 * dyj;
+    const float gy = t.s01 * dxi + t.s11 * dyj;
+    const float gz = t.s02 * dxi + t.s12 * dyj;
+    mom_cell<kClamp, 0, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
+    mom_cell<kClamp, 1, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
+    mom_cell<kClamp, 2, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
+}
+
+template <bool kClamp>
+__device__ __forceinline__ void mom_contrib_shared(const PW& w, const MomIn& in, const float* s, float coef,
+                                                   int32_t (*acc)[kHaloCells], int hb) {
+    MomTerms t;
+    t.s00 = s[0]; t.s11 = s[1]; t.s01 = s[3]; t.s02 = s[4]; t.s12 = s[5];
+    const float s22 = s[2];
+    t.coef = coef;
+    t.dxs[0] = -w.fx - 1.0f; t.dxs[1] = -w.fx; t.dxs[2] = 1.0f - w.fx;
+    t.dys[0] = -w.fy - 1.0f; t.dys[1] = -w.fy; t.dys[2] = 1.0f - w.fy;
+    const float dzs[3] = {-w.fz - 1.0f, -w.fz, 1.0f - w.fz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        t.qz[0][k] = in.a02 * dzs[k];
+        t.qz[1][k] = in.a12 * dzs[k];
+        t.qz[2][k] = in.a22 * dzs[k];
+        t.fz[0][k] = t.s02 * dzs[k];
+        t.fz[1][k] = t.s12 * dzs[k];
+        t.fz[2][k] = s22 * dzs[k];
+    }
+    int32_t* a0 = &acc[0][hb];
+    int32_t* a1 = &acc[1][hb];
+    int32_t* a2 = &acc[2][hb];
+    mom_column<kClamp, 0, 0>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 0, 1>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 0, 2>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 1, 0>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 1, 1>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 1, 2>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 2, 0>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 2, 1>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 2, 2>(w, in, t, a0, a1, a2);
+}
+
 // P2G_MOM for one particle whose inputs are loaded.
 __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr& h, const SceneDesc& sd, bool valid,
                                              uint32_t p, const float4 pm, const float4 vi, const float* a,
@@ -952,6 +1030,7 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
     bool leader;
     const uint32_t grp = agg_group(shared_path, hb, lane, leader);
     if (shared_path) {
+#if MPM_P2G_AGG
         auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
             const int hi = hb + k * kHXY + j * kHX + i;
             agg_add(&acc[0][hi], ex, grp, leader);
@@ -961,6 +1040,11 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
         // the clamp-free form only when the whole group can use it
         if (__all_sync(grp, safe)) mom_contrib<false>(w, in, s, coef, sink);
         else mom_contrib<true>(w, in, s, coef, sink);
+#else
+        (void)grp;
+        if (safe) mom_contrib_shared<false>(w, in, s, coef, acc, hb);
+        else mom_contrib_shared<true>(w, in, s, coef, acc, hb);
+#endif
     } else if (live) {
         auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
             const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
