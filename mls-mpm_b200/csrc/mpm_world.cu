@@ -622,6 +622,33 @@ __device__ __forceinline__ uint32_t agg_group(bool shared_path, int hb, uint32_t
 #endif
 }
 
+// The 27 P2G_MASS contributions of one particle into the shared halo at base
+// slot hb, written out through template indices (immediate offsets, no
+// per-cell control flow).  kClamp: encode with its clamp.
+template <bool kClamp, int K, int J, int I>
+__device__ __forceinline__ void mass_cell(const PW& w, float m, int32_t* a) {
+    const float x = w.wx[I] * w.wy[J] * w.wz[K] * m;
+    atomicAdd(a + (K * kHXY + J * kHX + I), kClamp ? encode(x) : encode_unclamped(x));
+}
+template <bool kClamp, int K, int J>
+__device__ __forceinline__ void mass_row(const PW& w, float m, int32_t* a) {
+    mass_cell<kClamp, K, J, 0>(w, m, a);
+    mass_cell<kClamp, K, J, 1>(w, m, a);
+    mass_cell<kClamp, K, J, 2>(w, m, a);
+}
+template <bool kClamp>
+__device__ __forceinline__ void mass_contrib_shared(const PW& w, float m, int32_t* a) {
+    mass_row<kClamp, 0, 0>(w, m, a);
+    mass_row<kClamp, 0, 1>(w, m, a);
+    mass_row<kClamp, 0, 2>(w, m, a);
+    mass_row<kClamp, 1, 0>(w, m, a);
+    mass_row<kClamp, 1, 1>(w, m, a);
+    mass_row<kClamp, 1, 2>(w, m, a);
+    mass_row<kClamp, 2, 0>(w, m, a);
+    mass_row<kClamp, 2, 1>(w, m, a);
+    mass_row<kClamp, 2, 2>(w, m, a);
+}
+
 // ---------------------------------------------------------------------------
 // P2G_MASS (shaders.js:242-274): one block per chunk, one thread per particle
 // ---------------------------------------------------------------------------
@@ -674,6 +701,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             if (fast) {
                 // weight <= 0.4219: for |mass| < 47000 encode's clamp is the identity
                 const bool safe = fabsf(q[r].w) < 47000.0f;
+#if MPM_P2G_AGG
 #pragma unroll
                 for (int kk = 0; kk < 3; ++kk)
 #pragma unroll
@@ -684,6 +712,11 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
                             const int32_t e = safe ? encode_unclamped(x) : encode(x);
                             agg_add(&acc[hb + kk * kHXY + j * kHX + i], e, grp, leader);
                         }
+#else
+                (void)grp;
+                if (safe) mass_contrib_shared<false>(w, q[r].w, acc + hb);
+                else mass_contrib_shared<true>(w, q[r].w, acc + hb);
+#endif
             } else if (valid) {
                 // stencil outside the halo or the grid: bounds-checked global atomics
                 const int32_t X = sd.X, Y = sd.Y, Z = sd.Z;
@@ -968,6 +1001,33 @@ __device__ __forceinline__ void mom_contrib_shared(const PW& w, const MomIn& in,
     mom_column<kClamp, 2, 2>(w, in, t, a0, a1, a2);
 }
 
+// Density of one particle from the staged halo masses (shaders.js:305-313):
+// the reference's k, j, i summation order, written out through template
+// indices.
+template <int K, int J, int I>
+__device__ __forceinline__ void density_term(const PW& w, const float* m, float& d) {
+    d += w.wx[I] * w.wy[J] * w.wz[K] * m[K * kHXY + J * kHX + I];
+}
+template <int K, int J>
+__device__ __forceinline__ void density_row(const PW& w, const float* m, float& d) {
+    density_term<K, J, 0>(w, m, d);
+    density_term<K, J, 1>(w, m, d);
+    density_term<K, J, 2>(w, m, d);
+}
+__device__ __forceinline__ float density_shared(const PW& w, const float* m) {
+    float d = 0.0f;
+    density_row<0, 0>(w, m, d);
+    density_row<0, 1>(w, m, d);
+    density_row<0, 2>(w, m, d);
+    density_row<1, 0>(w, m, d);
+    density_row<1, 1>(w, m, d);
+    density_row<1, 2>(w, m, d);
+    density_row<2, 0>(w, m, d);
+    density_row<2, 1>(w, m, d);
+    density_row<2, 2>(w, m, d);
+    return d;
+}
+
 // P2G_MOM for one particle whose inputs are loaded.
 __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr& h, const SceneDesc& sd, bool valid,
                                              uint32_t p, const float4 pm, const float4 vi, const float* a,
@@ -982,13 +1042,7 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
     // density (shaders.js:305-313), k, j, i order
     float density = 0.0f;
     if (fast) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-#pragma unroll
-            for (int jj = 0; jj < 3; ++jj)
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    density += w.wx[i] * w.wy[jj] * w.wz[k] * mh[hb + k * kHXY + jj * kHX + i];
+        density = density_shared(w, mh + hb);
     } else if (valid) {
         for (int k = 0; k < 3; ++k)
             for (int jj = 0; jj < 3; ++jj)
