@@ -13,6 +13,7 @@ particle-updates over the max-over-ranks device time ("scaling": "weak").
 import argparse
 import ctypes
 import json
+import math
 import os
 import statistics
 import sys
@@ -44,6 +45,11 @@ def measured_peaks():
 # i32 write 12), UPDATE_GRID 28 (momentum+mass read 16, velocity write 12),
 # G2P 12 (velocity read).  Sum: 180 B per particle + 60 B per cell.
 PHASE_BYTES = {"p2g_mass": (20, 4), "p2g_mom": (76, 16), "update_grid": (0, 28), "g2p": (84, 12)}
+
+# Bytes of one scene's uniform block in the device scene table (grid dims and
+# ranges, Params 80 B, WallParams 336 B, HandParams 80 B, hand box): what a
+# frame that changes any uniform uploads.
+SCENE_DESC_BYTES = 576
 
 
 class ClockSampler:
@@ -247,25 +253,30 @@ def main():
     names = [lib.mpm_phase_name(i).decode() for i in range(10)]
     fl.destroy()
 
-    # (3) end to end through the public API over the same substeps: per step
-    # the host writes the frame's uniforms (params, walls, hand:
-    # fluid-gpu.js:295-328, 337-413, 479-527) and reads back the diffuse alive
-    # count (diffuse-gpu.js:172-188), synchronously, like the reference's frame.
+    # (3) end to end through the public API over the same substeps, as the
+    # reference's frame drives it (main.js:504-528): per step the host moves
+    # the hand (fluid-gpu.js:479-527; a small cylinder sweeping the empty top
+    # corner of the domain, so every frame carries new uniforms, uploaded from
+    # pinned memory), steps the scene, queues the diffuse alive-count readback
+    # (diffuse-gpu.js:172-176) and polls it (178-188) without waiting; the
+    # clock stops after the last readback has landed.
     fl = make()
+    X, Y, Z = scene.grid
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        fl.updateHand([40.0, 60.0, 40.0], [0.0, 0.0, 0.0], 4.0, 1.0, False, [40.0, 60.0, 140.0])
-        fl._params_prev = None
-        fl._walls.prev_buf[:] = np.nan
+    for s in range(args.steps):
+        hz = Z - 14.0 + 2.0 * math.sin(0.1 * s)
+        fl.updateHand([X - 14.0, Y - 12.0, hz], [0.0, 0.0, 0.5], 3.0, 0.2, True, [X - 14.0, Y - 12.0, Z + 40.0])
         fl.simFrame()
         if fl.diffuse is not None:
+            fl.diffuse.requestDebugReadback()
             fl.diffuse.pollDebug()
-        else:
-            fl.sync()
+    fl.sync()
+    if fl.diffuse is not None:
+        fl.diffuse.pollDebug()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     fl.destroy()
-    h2d = 80 + 336 + 80
+    h2d = SCENE_DESC_BYTES   # the scene's uniform block, changed by the hand every frame
     d2h = 4 if scene.diffuse_max else 0
 
     n = scene.n

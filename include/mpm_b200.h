@@ -160,6 +160,18 @@ mpm_status mpm_upload(mpm_scene* scene, mpm_buffer which, const void* host_src, 
  * alive = maxCount - freeListTop.  Waits for the stream. */
 mpm_status mpm_diffuse_alive_count(mpm_scene* scene, int32_t* alive);
 
+/* DiffuseGPU.requestDebugReadback (diffuse-gpu.js:172-176), asynchronous: a
+ * 4-byte copy of freeListTop queued on the scene stream after the work
+ * already enqueued, into a ring of 4 pinned slots.  With every slot still in
+ * flight it first waits for the oldest one (so the host never runs more than
+ * 4 readbacks ahead of the device). */
+mpm_status mpm_diffuse_request_alive(mpm_scene* scene);
+
+/* DiffuseGPU.pollDebug (diffuse-gpu.js:178-188), non-blocking: reads every
+ * completed readback in order; *alive = maxCount - top of the newest one read
+ * so far (0 before the first), *ready = 1 if this call read at least one. */
+mpm_status mpm_diffuse_poll_alive(mpm_scene* scene, int32_t* alive, int32_t* ready);
+
 /* The scene's CUDA stream (cudaStream_t), for callers that order their own
  * work after a step. */
 mpm_status mpm_get_stream(mpm_scene* scene, void** stream);

@@ -117,6 +117,9 @@ static void free_scene(Scene& s) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s.diffuse.host_top) cudaFreeHost(s.diffuse.host_top);
+    if (s.diffuse.alive_ring) cudaFreeHost(s.diffuse.alive_ring);
+    for (cudaEvent_t& ev : s.diffuse.alive_ev)
+        if (ev) cudaEventDestroy(ev);
     if (s.edit_host) cudaFreeHost(s.edit_host);
     if (s.stream) cudaStreamDestroy(s.stream);
 }
@@ -430,6 +433,9 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     if (e == cudaSuccess) e = dalloc(&d.gen_dev, sizeof(mpm_gen_params));
     if (e == cudaSuccess) e = dalloc(&d.adv_dev, sizeof(mpm_advect_params));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&d.host_top, 16);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&d.alive_ring, DiffuseState::kAliveRing * 4);
+    for (uint32_t i = 0; i < DiffuseState::kAliveRing && e == cudaSuccess; ++i)
+        e = cudaEventCreateWithFlags(&d.alive_ev[i], cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_fail(e, "mpm_diffuse_enable allocation");
     // diffuse-gpu.js:60-68: free list [0..M-1], top = M, all slots dead
     std::vector<uint32_t> fl(M);
@@ -533,6 +539,46 @@ mpm_status mpm_diffuse_alive_count(mpm_scene* sc, int32_t* alive) {
     CUDA_TRY(cudaMemcpyAsync(d.host_top, d.top, 4, cudaMemcpyDeviceToHost, sc->s.stream), "top readback");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "top sync");
     *alive = (int32_t)d.max_count - *d.host_top;
+    return MPM_OK;
+}
+
+mpm_status mpm_diffuse_request_alive(mpm_scene* sc) {
+    if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    DiffuseState& d = sc->s.diffuse;
+    if (!d.enabled) return fail(MPM_ERR_INVALID_ARG, "diffuse not enabled");
+    DeviceGuard guard(sc->s.device);
+    constexpr uint32_t R = DiffuseState::kAliveRing;
+    if (d.alive_head - d.alive_tail == R) {   // every slot in flight: take the oldest
+        const uint32_t t = d.alive_tail % R;
+        CUDA_TRY(cudaEventSynchronize(d.alive_ev[t]), "alive readback wait");
+        d.alive_last = (int32_t)d.max_count - d.alive_ring[t];
+        ++d.alive_tail;
+    }
+    const uint32_t h = d.alive_head % R;
+    CUDA_TRY(cudaMemcpyAsync(d.alive_ring + h, d.top, 4, cudaMemcpyDeviceToHost, sc->s.stream), "alive readback");
+    CUDA_TRY(cudaEventRecord(d.alive_ev[h], sc->s.stream), "alive readback event");
+    ++d.alive_head;
+    return MPM_OK;
+}
+
+mpm_status mpm_diffuse_poll_alive(mpm_scene* sc, int32_t* alive, int32_t* ready) {
+    if (!sc || !alive || !ready) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    DiffuseState& d = sc->s.diffuse;
+    if (!d.enabled) return fail(MPM_ERR_INVALID_ARG, "diffuse not enabled");
+    DeviceGuard guard(sc->s.device);
+    constexpr uint32_t R = DiffuseState::kAliveRing;
+    int32_t got = 0;
+    while (d.alive_tail != d.alive_head) {
+        const uint32_t t = d.alive_tail % R;
+        const cudaError_t q = cudaEventQuery(d.alive_ev[t]);
+        if (q == cudaErrorNotReady) break;
+        if (q != cudaSuccess) return cuda_fail(q, "alive readback query");
+        d.alive_last = (int32_t)d.max_count - d.alive_ring[t];
+        ++d.alive_tail;
+        got = 1;
+    }
+    *alive = d.alive_last;
+    *ready = got;
     return MPM_OK;
 }
 

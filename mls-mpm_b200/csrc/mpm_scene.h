@@ -33,6 +33,13 @@ struct DiffuseState {
     int32_t* rank_state = nullptr;          // [0] = top before the pass, [1] = total, [2] = applied
     mpm_diffuse_particle* staging = nullptr;  // N x 48 B spawn records indexed by particle id
     int32_t* host_top = nullptr;            // pinned 4 B for alive-count readback
+    // asynchronous alive-count readbacks (requestDebugReadback / pollDebug):
+    // a ring of pinned slots, each with the event recorded after its copy
+    static constexpr uint32_t kAliveRing = 4;
+    int32_t* alive_ring = nullptr;          // pinned kAliveRing x 4 B
+    cudaEvent_t alive_ev[kAliveRing] = {};
+    uint32_t alive_head = 0, alive_tail = 0;   // next slot to fill / oldest unread
+    int32_t alive_last = 0;                 // latest value read back
     mpm_gen_params* gen_dev = nullptr;      // device GenParams (binned engine: seed bumped on the device)
     mpm_advect_params* adv_dev = nullptr;   // device copy of adv (binned engine)
 };

@@ -1718,6 +1718,11 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
     });
     if (e != cudaSuccess) return e;
     w.h_scenes.assign(scene_cap, SceneDesc{});
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+        e = cudaMallocHost((void**)&w.h_stage[b], (size_t)scene_cap * sizeof(SceneDesc));
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.stage_ev[b], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return e;
     w.h_tile_scene.assign(T, kHole);
     // zero everything the sparse passes rely on being zero
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) e = cudaMemsetAsync(w.grid_i32[b], 0, C * 16, stream);
@@ -1741,6 +1746,12 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
 
 void world_free(World& w) {
     if (w.stream) cudaStreamSynchronize(w.stream);
+    for (int b = 0; b < 2; ++b) {
+        if (w.h_stage[b]) cudaFreeHost(w.h_stage[b]);
+        if (w.stage_ev[b]) cudaEventDestroy(w.stage_ev[b]);
+        w.h_stage[b] = nullptr;
+        w.stage_ev[b] = nullptr;
+    }
     for (int b = 0; b < 2; ++b)
         if (w.graph[b]) cudaGraphExecDestroy(w.graph[b]);
     world_arrays(w, [](auto*& p, size_t) {
@@ -1778,10 +1789,19 @@ cudaError_t world_upload_table(World& w) {
         if (w.scenes[i].live) hi = i + 1;
     for (int i = 0; i < hi; ++i) fill_desc(w, i);
     cudaError_t e = cudaSuccess;
-    // pageable source: the copy is staged before the call returns, so the host
-    // table can change again right away without racing the queued copy
-    if (hi) e = cudaMemcpyAsync(w.d_scenes, w.h_scenes.data(), (size_t)hi * sizeof(SceneDesc),
-                                cudaMemcpyHostToDevice, w.stream);
+    if (hi) {
+        // pinned staging copy (an upload from pageable memory would first wait
+        // for all work queued on the stream); the copy it last fed must be done
+        const int b = w.stage_i;
+        w.stage_i ^= 1;
+        e = cudaEventSynchronize(w.stage_ev[b]);
+        if (e == cudaSuccess) {
+            std::memcpy(w.h_stage[b], w.h_scenes.data(), (size_t)hi * sizeof(SceneDesc));
+            e = cudaMemcpyAsync(w.d_scenes, w.h_stage[b], (size_t)hi * sizeof(SceneDesc), cudaMemcpyHostToDevice,
+                                w.stream);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(w.stage_ev[b], w.stream);
+    }
     if (e == cudaSuccess) w.table_dirty = false;
     return e;
 }

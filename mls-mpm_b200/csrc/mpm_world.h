@@ -52,6 +52,7 @@ struct alignas(16) SceneDesc {
     mpm_wall_params W;
     mpm_hand_params H;          // APPLY_HAND uniform, applied inside UPDATE_GRID over hand_box
 };
+static_assert(sizeof(SceneDesc) == 576, "bench.py SCENE_DESC_BYTES counts this block per uniform upload");
 
 // Small device-side control block.  The first kCtrlZeroBytes are cleared at
 // the start of every substep.
@@ -152,7 +153,13 @@ struct World {
 
     // device arrays
     SceneDesc* d_scenes = nullptr;
-    std::vector<SceneDesc> h_scenes;        // host copy of the table (pageable, see world_upload_table)
+    std::vector<SceneDesc> h_scenes;        // host copy of the table
+    // pinned staging copies of the table for asynchronous uploads (a copy from
+    // pageable memory would wait for the stream); each is reused only after
+    // the upload that last read it has completed (stage_ev)
+    SceneDesc* h_stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    int stage_i = 0;
     uint32_t* tile_scene = nullptr;
     std::vector<uint32_t> h_tile_scene;
     float4* posm[2] = {nullptr, nullptr};   // (x, y, z, mass)

@@ -171,6 +171,8 @@ SIGNATURES = {
     "mpm_download": (_I, [_V, _I, _V, _SZ]),
     "mpm_upload": (_I, [_V, _I, _V, _SZ]),
     "mpm_diffuse_alive_count": (_I, [_V, ctypes.POINTER(ctypes.c_int32)]),
+    "mpm_diffuse_request_alive": (_I, [_V]),
+    "mpm_diffuse_poll_alive": (_I, [_V, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "mpm_get_stream": (_I, [_V, ctypes.POINTER(_V)]),
     "mpm_phase_name": (ctypes.c_char_p, [_I]),
     "mpm_profile_enable": (_I, [_V, _I]),

@@ -309,10 +309,22 @@ class DiffuseGPU:
               "mpm_diffuse_set_gen_params")
 
     def requestDebugReadback(self, cmd=None):
-        pass
+        """diffuse-gpu.js:172-176: queue a copy of the free-list top after the
+        work submitted so far (asynchronous; a ring of 4 readbacks in flight)."""
+        check(self.fluid._lib.mpm_diffuse_request_alive(self.fluid._scene), "mpm_diffuse_request_alive")
 
     def pollDebug(self):
-        """diffuse-gpu.js:178-188: aliveCount = maxCount - top."""
+        """diffuse-gpu.js:178-188: aliveCount = maxCount - top once a requested
+        readback has landed; never waits.  Returns the current aliveCount."""
+        a, ready = ctypes.c_int32(), ctypes.c_int32()
+        check(self.fluid._lib.mpm_diffuse_poll_alive(self.fluid._scene, ctypes.byref(a), ctypes.byref(ready)),
+              "mpm_diffuse_poll_alive")
+        if ready.value:
+            self.aliveCount = a.value
+        return self.aliveCount
+
+    def readAliveCount(self):
+        """The alive count now (waits for the stream)."""
         a = ctypes.c_int32()
         check(self.fluid._lib.mpm_diffuse_alive_count(self.fluid._scene, ctypes.byref(a)),
               "mpm_diffuse_alive_count")

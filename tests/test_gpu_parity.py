@@ -79,5 +79,10 @@ def test_fluidgpu_class_drop_in(gpu):
         o = next(ref)
         assert np.array_equal(fl.read("pos"), o["pos"]), s
         assert np.array_equal(fl.read("cell_mass"), o["cell_mass"]), s
-    assert dif.pollDebug() == sc.diffuse_max - int(o["top"][0])
+    want = sc.diffuse_max - int(o["top"][0])
+    assert dif.readAliveCount() == want
+    # the asynchronous pair: a readback queued after the step, read once it landed
+    dif.requestDebugReadback()
+    fl.sync()
+    assert dif.pollDebug() == want
     fl.destroy()
