@@ -148,6 +148,17 @@ mpm_status mpm_sync(mpm_scene* scene);
  * renderer's vertex input, fluid-renderer.js:315-328). */
 mpm_status mpm_get_buffer(mpm_scene* scene, mpm_buffer which, void** dev_ptr, size_t* bytes);
 
+/* Zero-copy export of a buffer (reference layout) to another process on the
+ * same node, e.g. a renderer reading the particle positions, velocities and
+ * densities as vertex inputs (fluid-renderer.js:315-328) or the diffuse pool
+ * (850-856): `handle` receives the MPM_IPC_HANDLE_BYTES-byte CUDA IPC handle
+ * (cudaIpcMemHandle_t) of the device allocation that holds the buffer, and
+ * `offset` the buffer's byte offset in it.  The consumer opens the handle
+ * with cudaIpcOpenMemHandle.  Contents follow the same rules as
+ * mpm_get_buffer; order the consumer's reads after mpm_sync. */
+#define MPM_IPC_HANDLE_BYTES 64
+mpm_status mpm_get_ipc_handle(mpm_scene* scene, mpm_buffer which, void* handle, size_t* offset, size_t* bytes);
+
 /* Copy a buffer (reference layout) to host memory; waits for the stream.
  * `bytes` may be smaller than the buffer (a prefix is copied). */
 mpm_status mpm_download(mpm_scene* scene, mpm_buffer which, void* host_dst, size_t bytes);

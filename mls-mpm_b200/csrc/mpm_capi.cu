@@ -1,5 +1,6 @@
 // mpm_capi.cu — the C ABI (include/mpm_b200.h): scene lifetime, uploads,
 // uniforms, stepping and buffer export.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -499,6 +500,41 @@ mpm_status mpm_get_buffer(mpm_scene* sc, mpm_buffer which, void** dev_ptr, size_
         DeviceGuard guard(sc->s.device);
         CUDA_TRY(sync_reference_buffers(sc->s), "export");
     }
+    return MPM_OK;
+}
+
+// Base address of the device allocation that holds p (driver entry point
+// looked up at run time, so the library needs no link-time libcuda).
+static cudaError_t allocation_base(const void* p, CUdeviceptr* base, size_t* size) {
+    using RangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+    static RangeFn fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q);
+        if (e != cudaSuccess) return e;
+        if (q != cudaDriverEntryPointSuccess || !f) return cudaErrorSymbolNotFound;
+        fn = reinterpret_cast<RangeFn>(f);
+    }
+    return fn(base, size, reinterpret_cast<CUdeviceptr>(p)) == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+mpm_status mpm_get_ipc_handle(mpm_scene* sc, mpm_buffer which, void* handle, size_t* offset, size_t* bytes) {
+    if (!sc || !handle || !offset || !bytes) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    void* p;
+    size_t sz;
+    if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
+    DeviceGuard guard(sc->s.device);
+    if (is_particle_buffer(which)) CUDA_TRY(sync_reference_buffers(sc->s), "export");
+    CUdeviceptr base = 0;
+    size_t alloc = 0;
+    CUDA_TRY(allocation_base(p, &base, &alloc), "allocation range");
+    static_assert(sizeof(cudaIpcMemHandle_t) == MPM_IPC_HANDLE_BYTES, "IPC handle size");
+    cudaIpcMemHandle_t h;
+    CUDA_TRY(cudaIpcGetMemHandle(&h, reinterpret_cast<void*>(base)), "cudaIpcGetMemHandle");
+    std::memcpy(handle, &h, sizeof h);
+    *offset = (size_t)(reinterpret_cast<CUdeviceptr>(p) - base);
+    *bytes = sz;
     return MPM_OK;
 }
 

@@ -172,6 +172,8 @@ SIGNATURES = {
     "mpm_upload": (_I, [_V, _I, _V, _SZ]),
     "mpm_diffuse_alive_count": (_I, [_V, ctypes.POINTER(ctypes.c_int32)]),
     "mpm_diffuse_request_alive": (_I, [_V]),
+    "mpm_get_ipc_handle": (_I, [_V, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                                ctypes.POINTER(ctypes.c_size_t)]),
     "mpm_diffuse_poll_alive": (_I, [_V, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "mpm_get_stream": (_I, [_V, ctypes.POINTER(_V)]),
     "mpm_phase_name": (ctypes.c_char_p, [_I]),

@@ -240,6 +240,15 @@ class FluidGPU:
               "mpm_get_buffer")
         return p.value, sz.value
 
+    def get_ipc_handle(self, name):
+        """(handle bytes, offset, bytes) exporting a reference-layout buffer to
+        another process (cudaIpcOpenMemHandle on the handle, then + offset)."""
+        h = ctypes.create_string_buffer(64)
+        off, sz = ctypes.c_size_t(), ctypes.c_size_t()
+        check(self._lib.mpm_get_ipc_handle(self._scene, BUF[name], h, ctypes.byref(off), ctypes.byref(sz)),
+              "mpm_get_ipc_handle")
+        return h.raw, off.value, sz.value
+
     def read(self, name):
         """Download one buffer as a numpy array in the reference layout."""
         n, G = self.particle_num, self.grid_num
