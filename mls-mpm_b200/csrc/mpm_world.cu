@@ -522,6 +522,11 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, uint32_
     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
 }
+// Asynchronous 4-byte global -> shared copy; src_bytes 0 writes a zero.
+__device__ __forceinline__ void cp_async4z(void* smem, const void* gmem, uint32_t src_bytes) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
@@ -1115,110 +1120,110 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
 #ifndef MPM_G2P_MINB
 #define MPM_G2P_MINB 4
 #endif
-#ifndef MPM_MOM_PREFETCH
-#define MPM_MOM_PREFETCH 1
-#endif
+
 #ifndef MPM_MOM_MINB
 #define MPM_MOM_MINB 2
 #endif
 
+// P2G_MOM, software-pipelined across the block's chunks: while chunk c runs,
+// the halo masses of the block's next chunk are copied into the other
+// staging buffer (cp.async) and its first particle's inputs are loaded; the
+// accumulators are zeroed by the flush that reads them.
+__device__ __forceinline__ void stage_masses_async(const WorldView& v, const ChunkHdr& hh,
+                                                   const float* __restrict__ cmf, float* buf) {
+    const SceneDesc& nsd = v.scenes[hh.scene];
+    const float* src = cmf + nsd.cell_base;
+    const int hn = halo_span(hh);
+    for (int i = threadIdx.x; i < hn; i += blockDim.x) {
+        uint32_t cell;
+        const bool in = halo_cell(hh, nsd, i, cell);
+        cp_async4z(buf + i, in ? (const void*)(src + cell) : (const void*)src, in ? 4u : 0u);
+    }
+}
+
+__device__ __forceinline__ void mom_load(const WorldView& v, uint32_t p, bool valid, const float4* __restrict__ posm,
+                                         const float4* __restrict__ velid, const float* __restrict__ aff,
+                                         size_t plane, float4& pm, float4& vi, float* a) {
+    const uint32_t slot = valid ? v.perm[p] : 0u;
+    if (valid) {
+        pm = posm[slot];
+        vi = velid[slot];
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) a[e] = valid ? aff[e * plane + slot] : 0.0f;
+}
+
 __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(WorldView v, const float4* __restrict__ posm,
-                                                                     const float4* __restrict__ velid,
-                                                                     const float* __restrict__ aff,
-                                                                     const float* __restrict__ cmf,
-                                                                     int32_t* __restrict__ mv,
-                                                                     float* __restrict__ dens) {
+                                                                   const float4* __restrict__ velid,
+                                                                   const float* __restrict__ aff,
+                                                                   const float* __restrict__ cmf,
+                                                                   int32_t* __restrict__ mv,
+                                                                   float* __restrict__ dens) {
     constexpr int kPer = kChunk / kChunkThreads;
-    __shared__ float mh[kHaloCells];
+    __shared__ float mh[2][kHaloCells];
     __shared__ int32_t acc[3][kHaloCells];
+    __shared__ ChunkHdr hdr[2];
+    __shared__ SceneDesc ssd;
     const uint32_t nch = v.ctrl->total_chunks;
+    const uint32_t G = gridDim.x;
+    if (blockIdx.x >= nch) return;   // block-uniform
     const uint32_t lane = threadIdx.x & 31;
     const size_t plane = v.npos;
-    __shared__ ChunkHdr hs;
-    __shared__ SceneDesc ssd;
     uint32_t cached = kHole;
-    // chunk headers: the next one's words are loaded while this chunk runs
-    uint4 nh0 = make_uint4(0u, 0u, 0u, 0u), nh1 = nh0;
-    if (threadIdx.x == 0 && blockIdx.x < nch) hs = unpack_header(v.chunk_hdr[2ull * blockIdx.x], v.chunk_hdr[2ull * blockIdx.x + 1]);
-    for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        __syncthreads();
-        const ChunkHdr h = hs;
-        const uint32_t nxt = ch + gridDim.x;
-        if (threadIdx.x == 0 && nxt < nch) {
-            nh0 = v.chunk_hdr[2ull * nxt];
-            nh1 = v.chunk_hdr[2ull * nxt + 1];
+    uint4 nh0 = make_uint4(0u, 0u, 0u, 0u), nh1 = nh0;   // thread 0: the words of the chunk two ahead
+    if (threadIdx.x == 0) {
+        const uint32_t c0 = blockIdx.x, c1 = c0 + G;
+        hdr[0] = unpack_header(v.chunk_hdr[2ull * c0], v.chunk_hdr[2ull * c0 + 1]);
+        if (c1 < nch) hdr[1] = unpack_header(v.chunk_hdr[2ull * c1], v.chunk_hdr[2ull * c1 + 1]);
+    }
+    for (int i = threadIdx.x; i < kHaloCells; i += blockDim.x) {
+        acc[0][i] = 0;
+        acc[1][i] = 0;
+        acc[2][i] = 0;
+    }
+    __syncthreads();
+    stage_masses_async(v, hdr[0], cmf, mh[0]);
+    // the first particle's inputs
+    uint32_t p = hdr[0].first + chunk_lane_offset();
+    bool valid = p < hdr[0].end;
+    float4 pm = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vi = pm;
+    float a[9];
+    mom_load(v, p, valid, posm, velid, aff, plane, pm, vi, a);
+    cp_async_wait();
+    __syncthreads();
+    int b = 0;
+    for (uint32_t ch = blockIdx.x; ch < nch; ch += G) {
+        const ChunkHdr h = hdr[b];
+        const uint32_t nxt = ch + G, nxt2 = nxt + G;
+        if (threadIdx.x == 0 && nxt2 < nch) {
+            nh0 = v.chunk_hdr[2ull * nxt2];
+            nh1 = v.chunk_hdr[2ull * nxt2 + 1];
         }
         load_scene(v, h.scene, ssd, cached);
         const SceneDesc& sd = ssd;
         const float* scmf = cmf + sd.cell_base;
         int32_t* smv = mv + 3ull * sd.cell_base;
-        // the first particle's inputs are in flight while the halo is staged
-        uint32_t p = h.first + chunk_lane_offset();
-        bool valid = p < h.end;
-        float4 pm = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vi = pm;
-        float a[9];
-        {
-            const uint32_t slot = valid ? v.perm[p] : 0u;
-            if (valid) {
-                pm = posm[slot];
-                vi = velid[slot];
-            }
-#pragma unroll
-            for (int e = 0; e < 9; ++e) a[e] = valid ? aff[e * plane + slot] : 0.0f;
-        }
-        const int hn = halo_span(h);
-        {
-            // every load of the staging in flight before the first store
-            constexpr int kIt = (kHaloCells + kChunkThreads - 1) / kChunkThreads;
-            float m[kIt];
-#pragma unroll
-            for (int it = 0; it < kIt; ++it) {
-                const int i = threadIdx.x + it * kChunkThreads;
-                uint32_t cell;
-                m[it] = (i < hn && halo_cell(h, sd, i, cell)) ? scmf[cell] : 0.0f;
-            }
-#pragma unroll
-            for (int it = 0; it < kIt; ++it) {
-                const int i = threadIdx.x + it * kChunkThreads;
-                if (i < hn) {
-                    mh[i] = m[it];
-                    acc[0][i] = 0;
-                    acc[1][i] = 0;
-                    acc[2][i] = 0;
-                }
-            }
-        }
-        __syncthreads();
+        // the next chunk's halo masses, copied while this chunk runs
+        const bool has_next = nxt < nch;
+        if (has_next) stage_masses_async(v, hdr[b ^ 1], cmf, mh[b ^ 1]);
+        const uint32_t next_first = has_next ? hdr[b ^ 1].first : 0u, next_end = has_next ? hdr[b ^ 1].end : 0u;
 #pragma unroll 1
         for (int r = 0; r < kPer; ++r) {
-            // next particle's inputs
-            const uint32_t pn = p + kChunkThreads;
-            const bool vn = r + 1 < kPer && pn < h.end;
-            float4 pmn = pm, vin = vi;
+            // inputs of this thread's next particle: the next one of this
+            // chunk, or the first one of the block's next chunk
+            uint32_t pn;
+            bool vn;
+            if (r + 1 < kPer) {
+                pn = p + kChunkThreads;
+                vn = pn < h.end;
+            } else {
+                pn = next_first + chunk_lane_offset();
+                vn = has_next && pn < next_end;
+            }
+            float4 pmn = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vin = pmn;
             float an[9];
-#if MPM_MOM_PREFETCH
-            {
-                const uint32_t slot = vn ? v.perm[pn] : 0u;
-                if (vn) {
-                    pmn = posm[slot];
-                    vin = velid[slot];
-                }
-#pragma unroll
-                for (int e = 0; e < 9; ++e) an[e] = vn ? aff[e * plane + slot] : 0.0f;
-            }
-#endif
-            mom_particle(v, h, sd, valid, p, pm, vi, a, mh, acc, scmf, smv, dens, lane);
-#if !MPM_MOM_PREFETCH
-            {
-                const uint32_t slot = vn ? v.perm[pn] : 0u;
-                if (vn) {
-                    pmn = posm[slot];
-                    vin = velid[slot];
-                }
-#pragma unroll
-                for (int e = 0; e < 9; ++e) an[e] = vn ? aff[e * plane + slot] : 0.0f;
-            }
-#endif
+            mom_load(v, pn, vn, posm, velid, aff, plane, pmn, vin, an);
+            mom_particle(v, h, sd, valid, p, pm, vi, a, mh[b], acc, scmf, smv, dens, lane);
             p = pn;
             valid = vn;
             pm = pmn;
@@ -1227,18 +1232,26 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
             for (int e = 0; e < 9; ++e) a[e] = an[e];
         }
         __syncthreads();
+        // hdr[b] is free: the header two chunks ahead goes there
+        if (threadIdx.x == 0 && nxt2 < nch) hdr[b] = unpack_header(nh0, nh1);
+        const int hn = halo_span(h);
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
             const int32_t a0 = acc[0][i], a1 = acc[1][i], a2 = acc[2][i];
+            if ((a0 | a1 | a2) == 0) continue;
+            acc[0][i] = 0;
+            acc[1][i] = 0;
+            acc[2][i] = 0;
             uint32_t cell;
-            if ((a0 | a1 | a2) != 0 && halo_cell(h, sd, i, cell)) {
+            if (halo_cell(h, sd, i, cell)) {
                 int32_t* d = smv + 3ull * cell;
                 if (a0) atomicAdd(d + 0, a0);
                 if (a1) atomicAdd(d + 1, a1);
                 if (a2) atomicAdd(d + 2, a2);
             }
         }
+        cp_async_wait();
         __syncthreads();
-        if (threadIdx.x == 0 && nxt < nch) hs = unpack_header(nh0, nh1);
+        b ^= 1;
     }
 }
 
