@@ -671,8 +671,10 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     uint32_t nlast = 0;
     if (threadIdx.x == 0 && blockIdx.x < nch)
         chunk_header_from(v.chunk_info[blockIdx.x], v.chunk_last[blockIdx.x], v.chunk_geo[blockIdx.x], hs);
+    // the accumulators start at zero and every flush zeroes what it read
+    for (int i = threadIdx.x; i < kHaloCells; i += blockDim.x) acc[i] = 0;
+    __syncthreads();
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        __syncthreads();
         const ChunkHdr h = hs;
         const uint32_t nxt = ch + gridDim.x;
         if (threadIdx.x == 0) {
@@ -683,17 +685,15 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
                 ngeo = v.chunk_geo[nxt];
             }
         }
-        load_scene(v, h.scene, ssd, cached);
-        // this thread's particles, in flight while the halo is cleared
+        // this thread's particles, in flight while the scene descriptor loads
         float4 q[kPer];
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
             const uint32_t p = h.first + r * kChunkThreads + chunk_lane_offset();
             q[r] = p < h.end ? posm[v.perm[p]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
+        load_scene(v, h.scene, ssd, cached);
         const int hn = halo_span(h);
-        for (int i = threadIdx.x; i < hn; i += blockDim.x) acc[i] = 0;
-        __syncthreads();
         const SceneDesc& sd = ssd;
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
@@ -737,14 +737,17 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             }
         }
         __syncthreads();
+        // every thread holds this chunk's header: the next one can replace it
+        if (threadIdx.x == 0 && nxt < nch) chunk_header_from(nci, nlast, ngeo, hs);
         int32_t* scm = cm + sd.cell_base;
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
             const int32_t a = acc[i];
+            if (a == 0) continue;
+            acc[i] = 0;
             uint32_t cell;
-            if (a != 0 && halo_cell(h, sd, i, cell)) atomicAdd(&scm[cell], a);
+            if (halo_cell(h, sd, i, cell)) atomicAdd(&scm[cell], a);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && nxt < nch) chunk_header_from(nci, nlast, ngeo, hs);
     }
 }
 
@@ -1544,8 +1547,8 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     const float ke_threshold = dv.enabled ? dv.gen->ke_threshold : 0.0f;
     // chunk headers: the next one's words are copied while this chunk runs
     if (threadIdx.x == 0 && blockIdx.x < nch) hs = unpack_header(v.chunk_hdr[2ull * blockIdx.x], v.chunk_hdr[2ull * blockIdx.x + 1]);
+    __syncthreads();
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        __syncthreads();
         const ChunkHdr h = hs;
         const uint32_t nxt = ch + gridDim.x;
         if (threadIdx.x == 0 && nxt < nch) {
@@ -1579,6 +1582,11 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         }
         cp_async_wait();
         __syncthreads();
+        // every thread holds this chunk's header: the next one can replace it
+        if (threadIdx.x == 0 && nxt < nch) {
+            cp_async_wait();
+            hs = unpack_header(nhs[0], nhs[1]);
+        }
         const bool spawn_scene = dv.enabled && h.scene == dv.scene;
         const G2POut out{posm_out, velid_out, aff_out, plane, v.key, v.rank, v.cell_count, v.tile_flags, v.dens,
                          cmf + sd.cell_base, spawn_scene ? dv.gen : nullptr, bubble_min, pressure_threshold,
@@ -1628,10 +1636,6 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
             pend_rank = rk;
         }
         __syncthreads();
-        if (threadIdx.x == 0 && nxt < nch) {
-            cp_async_wait();
-            hs = unpack_header(nhs[0], nhs[1]);
-        }
     }
     if (pend_p != kHole) v.rank[pend_p] = pend_rank;
 }
