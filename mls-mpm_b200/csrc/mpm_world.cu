@@ -2,21 +2,27 @@
 //
 // Same arithmetic as mpm_kernels.cu (and so the same bits), organised for
 // the B200:
-//   * Particles are sorted by (tile, cell) every substep (counting sort:
-//     per-cell ranks, a scan per 16x8x8-cell tile, a two-level scan over
-//     tiles) and each tile's particles are cut into chunks of up to kChunk
-//     consecutive particles.  The new layout reads the previous one through
-//     a permutation (new position -> previous position), which stays nearly
-//     coalesced because the order changes little between substeps.
-//   * P2G_MASS, P2G_MOM and G2P run one block per chunk, one thread per
-//     particle.  A chunk's cells form a box inside its tile; P2G sums the
-//     i32 contributions of the box plus a one-cell halo in shared memory —
-//     lanes whose particles share a cell first add their values with one
-//     warp reduction (integer adds commute, so the bits equal the
-//     reference's atomics) — and flushes each halo cell to the grid with one
-//     atomic.  G2P stages the halo's grid velocities in shared memory and
-//     gathers from there.  Particles whose stencil leaves the halo or the
-//     grid take a direct path with the reference's own indexing.
+//   * Particles are sorted by (tile, cell) every substep (counting sort: the
+//     rank of each particle in its new cell is taken in G2P, then a scan per
+//     16x8x8-cell tile and a two-level scan over tiles) and each tile's
+//     particles are cut into chunks of up to kChunk consecutive particles.
+//     The new layout reads the previous one through a permutation (new
+//     position -> previous position), which stays nearly coalesced because
+//     the order changes little between substeps.
+//   * P2G_MASS, P2G_MOM and G2P run one 256-thread block per chunk, two
+//     particles per thread.  A chunk's cells form a box inside its tile; P2G
+//     sums the i32 contributions of the box plus a one-cell halo in shared
+//     memory (integer adds commute, so the bits equal the reference's global
+//     atomics) and flushes each halo cell to the grid with one atomic.  G2P
+//     stages the halo's grid velocities in shared memory and gathers from
+//     there.  The halo arrays use fixed strides, so a particle's 27 stencil
+//     offsets are compile-time immediates; the contribution loops are written
+//     out through template indices.  Particles whose stencil leaves the halo
+//     or the grid take a direct path with the reference's own indexing.
+//   * Latency hiding: each block keeps its chunk's scene descriptor in shared
+//     memory, loads the next chunk's header (packed by P2G_MASS) a chunk
+//     ahead, and P2G_MOM copies the next chunk's halo masses (cp.async) and
+//     loads its first particle while the current chunk runs.
 //   * Scenes: cells, tiles and particle ids of every scene are ranges of the
 //     world's arrays; a tile maps to its scene, and each kernel reads the
 //     scene's grid dims, params, walls and hand from the device scene table.
@@ -28,7 +34,10 @@
 //     buffer (s+1)%2, which is the CLEAR of s+1.  APPLY_HAND runs inside the
 //     UPDATE_GRID pass.
 //   * The diffuse spawn decision runs in the G2P epilogue (post-G2P pos/vel,
-//     this substep's density), staging records by particle id.
+//     this substep's density), staging records by particle id; G2P also
+//     counts the spawners per group of ids for the free-list ranking.
+//   * A substep (diffuse update included) is captured once per layout parity
+//     as a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -458,26 +467,12 @@ __device__ __forceinline__ int32_t encode_unclamped(float v) { return __float2in
 // ---------------------------------------------------------------------------
 // Chunks: the halo box of a chunk's cells in shared memory
 // ---------------------------------------------------------------------------
-// Shared-memory accumulation strategy of the P2G chunk kernels:
-//   MPM_P2G_AGG 1: lanes with the same stencil add their values with one warp
-//                  reduction, one lane adds the sum; 0: every lane adds its own.
-//   MPM_P2G_SPREAD 1: within each pass over the chunk, lane l of warp w takes
-//                  particle 8*l + w (neighbouring lanes in different cells, so
-//                  the lanes of one shared atomic rarely share an address);
-//                  0: lane order = particle order.
-#ifndef MPM_P2G_AGG
-#define MPM_P2G_AGG 0
-#endif
-#ifndef MPM_P2G_SPREAD
-#define MPM_P2G_SPREAD 1
-#endif
-
+// Lane layout of the P2G chunk kernels: within each pass over the chunk, lane
+// l of warp w takes particle 8*l + w, so neighbouring lanes sit in different
+// cells and the lanes of one shared atomic rarely share an address.  (Adding
+// same-cell lanes with a warp reduction first was measured 5x slower.)
 __device__ __forceinline__ uint32_t chunk_lane_offset() {
-#if MPM_P2G_SPREAD
     return (threadIdx.x & 31u) * (kChunkThreads / 32) + (threadIdx.x >> 5);
-#else
-    return threadIdx.x;
-#endif
 }
 
 struct ChunkHdr {
@@ -599,34 +594,6 @@ __device__ __forceinline__ bool halo_cell(const ChunkHdr& h, const SceneDesc& sd
     return true;
 }
 
-// Add into a shared accumulator (wrapping i32, as the reference's atomics).
-// Aggregated: lanes of `grp` (same stencil base) sum their values with one
-// warp reduction and one lane adds the sum.
-__device__ __forceinline__ void agg_add(int32_t* slot, int32_t val, uint32_t grp, bool leader) {
-#if MPM_P2G_AGG
-    const int32_t s = __reduce_add_sync(grp, val);
-    if (leader) atomicAdd(slot, s);
-#else
-    (void)grp;
-    (void)leader;
-    atomicAdd(slot, val);
-#endif
-}
-
-// Lanes sharing a stencil base (aggregated mode only).
-__device__ __forceinline__ uint32_t agg_group(bool shared_path, int hb, uint32_t lane, bool& leader) {
-#if MPM_P2G_AGG
-    const uint32_t grp = __match_any_sync(0xffffffffu, shared_path ? (uint32_t)hb : 0x80000000u + lane);
-    leader = (uint32_t)(__ffs(grp) - 1) == lane;
-    return grp;
-#else
-    (void)shared_path;
-    (void)hb;
-    leader = true;
-    return 1u << lane;
-#endif
-}
-
 // The 27 P2G_MASS contributions of one particle into the shared halo at base
 // slot hb, written out through template indices (immediate offsets, no
 // per-cell control flow).  kClamp: encode with its clamp.
@@ -662,7 +629,6 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     constexpr int kPer = kChunk / kChunkThreads;
     __shared__ int32_t acc[kHaloCells];
     const uint32_t nch = v.ctrl->total_chunks;
-    const uint32_t lane = threadIdx.x & 31;
     __shared__ ChunkHdr hs;
     __shared__ SceneDesc ssd;
     uint32_t cached = kHole;
@@ -701,27 +667,11 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             const PW w = particle_weights(q[r].x, q[r].y, q[r].z);
             const bool fast = valid && in_halo(w, h, sd);
             const int hb = halo_base(h, w.cx, w.cy, w.cz);
-            bool leader;
-            const uint32_t grp = agg_group(fast, hb, lane, leader);
             if (fast) {
                 // weight <= 0.4219: for |mass| < 47000 encode's clamp is the identity
                 const bool safe = fabsf(q[r].w) < 47000.0f;
-#if MPM_P2G_AGG
-#pragma unroll
-                for (int kk = 0; kk < 3; ++kk)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const float x = w.wx[i] * w.wy[j] * w.wz[kk] * q[r].w;
-                            const int32_t e = safe ? encode_unclamped(x) : encode(x);
-                            agg_add(&acc[hb + kk * kHXY + j * kHX + i], e, grp, leader);
-                        }
-#else
-                (void)grp;
                 if (safe) mass_contrib_shared<false>(w, q[r].w, acc + hb);
                 else mass_contrib_shared<true>(w, q[r].w, acc + hb);
-#endif
             } else if (valid) {
                 // stencil outside the halo or the grid: bounds-checked global atomics
                 const int32_t X = sd.X, Y = sd.Y, Z = sd.Z;
@@ -1041,7 +991,7 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
                                              uint32_t p, const float4 pm, const float4 vi, const float* a,
                                              const float* mh, int32_t (*acc)[kHaloCells],
                                              const float* __restrict__ scmf, int32_t* __restrict__ smv,
-                                             float* __restrict__ dens, uint32_t lane) {
+                                             float* __restrict__ dens) {
     const uint32_t X = sd.X, SLICE = sd.X * sd.Y, G = sd.G;
     const PW w = particle_weights(pm.x, pm.y, pm.z);
     const bool fast = valid && in_halo(w, h, sd);
@@ -1088,25 +1038,9 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
     const float bz = am * (fabsf(in.vz) + 1.5f * (fabsf(in.a20) + fabsf(in.a21) + fabsf(in.a22))) +
                      ac * 1.5f * (fabsf(s[4]) + fabsf(s[5]) + fabsf(s[2]));
     const bool safe = fmaxf(bx, fmaxf(by, bz)) * 0.4222f < 19000.0f;
-    const bool shared_path = live && fast;
-    bool leader;
-    const uint32_t grp = agg_group(shared_path, hb, lane, leader);
-    if (shared_path) {
-#if MPM_P2G_AGG
-        auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
-            const int hi = hb + k * kHXY + j * kHX + i;
-            agg_add(&acc[0][hi], ex, grp, leader);
-            agg_add(&acc[1][hi], ey, grp, leader);
-            agg_add(&acc[2][hi], ez, grp, leader);
-        };
-        // the clamp-free form only when the whole group can use it
-        if (__all_sync(grp, safe)) mom_contrib<false>(w, in, s, coef, sink);
-        else mom_contrib<true>(w, in, s, coef, sink);
-#else
-        (void)grp;
+    if (live && fast) {
         if (safe) mom_contrib_shared<false>(w, in, s, coef, acc, hb);
         else mom_contrib_shared<true>(w, in, s, coef, acc, hb);
-#endif
     } else if (live) {
         auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
             const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
@@ -1170,7 +1104,6 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
     const uint32_t nch = v.ctrl->total_chunks;
     const uint32_t G = gridDim.x;
     if (blockIdx.x >= nch) return;   // block-uniform
-    const uint32_t lane = threadIdx.x & 31;
     const size_t plane = v.npos;
     uint32_t cached = kHole;
     uint4 nh0 = make_uint4(0u, 0u, 0u, 0u), nh1 = nh0;   // thread 0: the words of the chunk two ahead
@@ -1226,7 +1159,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
             float4 pmn = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vin = pmn;
             float an[9];
             mom_load(v, pn, vn, posm, velid, aff, plane, pmn, vin, an);
-            mom_particle(v, h, sd, valid, p, pm, vi, a, mh[b], acc, scmf, smv, dens, lane);
+            mom_particle(v, h, sd, valid, p, pm, vi, a, mh[b], acc, scmf, smv, dens);
             p = pn;
             valid = vn;
             pm = pmn;
@@ -1282,14 +1215,9 @@ __device__ __forceinline__ bool estimate_normal_f(const float* __restrict__ cmf,
 
 // Spawn decision + staging (shaders.js:800-855), out of line: most particles
 // fail the density test that the caller applies first.
-#ifndef MPM_G2P_RARE_INLINE
-#define MPM_G2P_RARE_INLINE 0
-#endif
-#if MPM_G2P_RARE_INLINE
-#define MPM_G2P_RARE __forceinline__
-#else
+// Out-of-line functions for G2P's rare paths (keeps their registers out of
+// the common path).
 #define MPM_G2P_RARE __noinline__
-#endif
 // The spawn test's terms that need no neighbour data (shaders.js:807-815):
 // speed, kinetic energy and trapped air.
 struct SpawnPre {
