@@ -266,7 +266,9 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t x, uint32
 // then y, then z): exclusive scan of the cell counts inside the tile ->
 // cell_start (tile-local), tile total -> tile_cnt.  Also marks every tile the
 // particles' 3x3x3 stencils touch (bit 1).
-__global__ void __launch_bounds__(kTileCells) k_bin_cells(WorldView v) {
+__device__ void tiles_fold(const WorldView& v, mpm_gen_params* gen);
+
+__global__ void __launch_bounds__(kTileCells) k_bin_cells(WorldView v, mpm_gen_params* gen, int fold) {
     __shared__ uint32_t ws[33];
     __shared__ uint32_t dirs;
     const uint32_t nocc = v.ctrl->n_occ;
@@ -312,15 +314,27 @@ __global__ void __launch_bounds__(kTileCells) k_bin_cells(WorldView v) {
         }
         __syncthreads();
     }
+    if (!fold) return;
+    // the last block to finish runs the per-tile passes (block-uniform test)
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&v.ctrl->bins_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    tiles_fold(v, gen);
 }
 
 // Grid-tile list (stencil tiles of this substep or the last one, plus the
 // hand boxes); shifts the flags for the next substep.
-__global__ void k_tiles_grid(WorldView v) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= v.ntiles) return;
+// (The flags are read past L1: in the folded form other blocks of the same
+// kernel have just set their bit 1.)
+__device__ __forceinline__ void tile_grid_entry(const WorldView& v, uint32_t t) {
     const uint32_t scene = v.tile_scene[t];
-    const uint32_t f = v.tile_flags[t];
+    const uint32_t f = __ldcg(v.tile_flags + t);
     if (scene == kHole) {
         if (f) v.tile_flags[t] = 0u;
         return;
@@ -338,6 +352,11 @@ __global__ void k_tiles_grid(WorldView v) {
     const bool prev = (f & 4u) != 0;
     if (now || prev) v.tile_grid_list[atomicAdd(&v.ctrl->n_grid, 1u)] = t;
     if (f != (now ? 4u : 0u)) v.tile_flags[t] = now ? 4u : 0u;
+}
+
+__global__ void k_tiles_grid(WorldView v) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < v.ntiles) tile_grid_entry(v, t);
 }
 
 
@@ -381,6 +400,46 @@ __global__ void __launch_bounds__(1024) k_tile_scan_top(WorldView v, mpm_gen_par
         }
         cp += tp;
         cc += tc;
+    }
+    if (threadIdx.x == 0) {
+        v.ctrl->prev_total_pos = v.ctrl->total_pos;
+        v.ctrl->total_pos = min(cp, v.npos);
+        v.ctrl->total_chunks = min(cc, v.chunk_cap);
+        if (gen) gen->seed = gen->seed + 1u;
+    }
+}
+
+// Tiles of a world small enough for one block to finish the binning's
+// per-tile passes: the last k_bin_cells block to finish builds the grid-tile
+// list and scans the tile counts itself instead of three more launches.
+constexpr uint32_t kFoldTiles = 4096;
+
+// The grid-tile list and the exclusive scans of the particle and chunk counts
+// over all tiles (tile_pstart/tile_cstart global, group offsets 0), the layout
+// totals and the diffuse seed bump: the work of k_tiles_grid,
+// k_tile_scan_local and k_tile_scan_top, by one 1024-thread block.
+__device__ void tiles_fold(const WorldView& v, mpm_gen_params* gen) {
+    __shared__ uint32_t ws[33];
+    for (uint32_t t = threadIdx.x; t < v.ntiles; t += blockDim.x) tile_grid_entry(v, t);
+    uint32_t cp = 0, cc = 0;
+    for (uint32_t t0 = 0; t0 < v.ntiles; t0 += 1024) {
+        const uint32_t t = t0 + threadIdx.x;
+        // tile counts written by the other blocks of k_bin_cells: read past L1
+        const uint32_t np = (t < v.ntiles && v.tile_occ[t]) ? __ldcg(v.tile_cnt + t) : 0u;
+        const uint32_t nc = (np + kChunk - 1) / kChunk;
+        uint32_t tp, tc;
+        const uint32_t rp = block_exclusive_scan_1024(np, ws, tp);
+        const uint32_t rc = block_exclusive_scan_1024(nc, ws, tc);
+        if (t < v.ntiles) {
+            v.tile_pstart[t] = cp + rp;
+            v.tile_cstart[t] = cc + rc;
+        }
+        cp += tp;
+        cc += tc;
+    }
+    for (uint32_t g = threadIdx.x; g < v.ngroups; g += blockDim.x) {
+        v.group_pstart[g] = 0u;
+        v.group_cstart[g] = 0u;
     }
     if (threadIdx.x == 0) {
         v.ctrl->prev_total_pos = v.ctrl->total_pos;
@@ -1926,13 +1985,20 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
             w.launches++;
         }
         k_tiles_occ<<<ntb, 256, 0, st>>>(v);
-        k_bin_cells<<<w.bin_blocks, kTileCells, 0, st>>>(v);
-        k_tiles_grid<<<ntb, 256, 0, st>>>(v);
-        k_tile_scan_local<<<v.ngroups, 1024, 0, st>>>(v);
-        k_tile_scan_top<<<1, 1024, 0, st>>>(v, gen_dev);
+        if (v.ntiles <= kFoldTiles) {
+            // the last binning block builds the grid list and scans the tiles
+            k_bin_cells<<<w.bin_blocks, kTileCells, 0, st>>>(v, gen_dev, 1);
+            w.launches += 1;
+        } else {
+            k_bin_cells<<<w.bin_blocks, kTileCells, 0, st>>>(v, gen_dev, 0);
+            k_tiles_grid<<<ntb, 256, 0, st>>>(v);
+            k_tile_scan_local<<<v.ngroups, 1024, 0, st>>>(v);
+            k_tile_scan_top<<<1, 1024, 0, st>>>(v, gen_dev);
+            w.launches += 4;
+        }
         k_tile_finish<<<w.bin_blocks, kTileCells, 0, st>>>(v);
         k_scatter<<<nposb, 256, 0, st>>>(v);
-        w.launches += 7;
+        w.launches += 3;
     }
     {
         Phase ph(prof, MPM_PHASE_P2G_MASS);

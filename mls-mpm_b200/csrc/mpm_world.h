@@ -57,7 +57,7 @@ static_assert(sizeof(SceneDesc) == 576, "bench.py SCENE_DESC_BYTES counts this b
 // Small device-side control block.  The first kCtrlZeroBytes are cleared at
 // the start of every substep.
 struct Ctrl {
-    uint32_t n_occ, n_grid, pad0, pad1;
+    uint32_t n_occ, n_grid, bins_done, pad1;   // bins_done: k_bin_cells blocks finished
     // persistent
     uint32_t total_chunks;      // chunks of the current layout
     uint32_t total_pos;         // positions of the current layout
