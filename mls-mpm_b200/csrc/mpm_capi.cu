@@ -445,6 +445,7 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     CUDA_TRY(cudaMemcpyAsync(d.free_list, fl.data(), M * 4, cudaMemcpyHostToDevice, s.stream), "free list");
     CUDA_TRY(cudaMemcpyAsync(d.top, &top, 4, cudaMemcpyHostToDevice, s.stream), "top");
     CUDA_TRY(cudaMemsetAsync(d.pool, 0, M * 48, s.stream), "pool");
+    CUDA_TRY(cudaMemsetAsync(d.rank_state, 0, 16, s.stream), "free-list pass state");
     CUDA_TRY(cudaStreamSynchronize(s.stream), "diffuse init sync");
     d.max_count = (uint32_t)M;
     d.gen = *gen;

@@ -14,6 +14,7 @@
 // keep the reference's invariant and never touches memory outside the buffer.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "mpm_device.cuh"
@@ -438,103 +439,10 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_gen_eval(const float4* __r
     }
 }
 
-// Exclusive scan of the group counts (one block).  Applies the pass to the
-// free-list top: mode 0 (spawn) pops min(total, top) slots when top > 0,
-// mode 1 (kill) pushes total slots.  state = {top before, total, applied}.
-__global__ void __launch_bounds__(1024) k_rank_scan(uint32_t* __restrict__ counts, uint32_t nb,
-                                                     int32_t* __restrict__ top, int32_t* __restrict__ state,
-                                                     int mode) {
-    __shared__ uint32_t ws[32];
-    __shared__ uint32_t carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (uint32_t base = 0; base < nb; base += 1024) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < nb ? counts[i] : 0u;
-        uint32_t x = v;
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) ws[wid] = x;
-        __syncthreads();
-        if (wid == 0) {
-            uint32_t s = ws[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-                if (lane >= o) s += y;
-            }
-            ws[lane] = s;
-        }
-        __syncthreads();
-        const uint32_t excl = carry + (wid > 0 ? ws[wid - 1] : 0u) + x - v;
-        if (i < nb) counts[i] = excl;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += ws[31];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const int32_t t0 = *top;
-        const int32_t total = (int32_t)carry;
-        int32_t applied;
-        if (mode == 0) {
-            applied = t0 > 0 ? (total < t0 ? total : t0) : 0;
-            *top = t0 - applied;
-        } else {
-            applied = total;
-            *top = t0 + total;
-        }
-        state[0] = t0; state[1] = total; state[2] = applied;
-    }
-}
-
-// Rank of this thread's bit among the set bits of its group (kGroupIds ids,
-// one per thread of a 256-thread block; warp k holds word k of the group),
-// in ascending id order.  bit: whether this thread's bit is set.
-__device__ __forceinline__ uint32_t group_bit_rank(uint32_t word, bool& bit) {
-    __shared__ uint32_t wc[kGroupIds / 32];
-    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-    if (lane == 0) wc[wid] = __popc(word);
-    __syncthreads();
-    uint32_t pre = 0;
-    for (uint32_t k = 0; k < wid; ++k) pre += wc[k];
-    bit = (word >> lane) & 1u;
-    return pre + __popc(word & ((1u << lane) - 1u));
-}
-
-// Spawners in ascending id take free-list slots top-1, top-2, ...: the
-// spawner of rank r takes free_list[top-1-r] if r < applied.  One block per
-// group of kGroupIds ids (counts: exclusive group offsets from k_rank_scan,
-// state[1] the total); groups without spawners return at once.
-__global__ void __launch_bounds__(kGroupIds) k_spawn_write(const uint32_t* __restrict__ bits, uint32_t n,
-                                                           const uint32_t* __restrict__ counts,
-                                                           const int32_t* __restrict__ state,
-                                                           const uint32_t* __restrict__ free_list,
-                                                           const mpm_diffuse_particle* __restrict__ staging,
-                                                           mpm_diffuse_particle* __restrict__ pool, uint32_t M) {
-    const uint32_t g = blockIdx.x, ng = (n + kGroupIds - 1) / kGroupIds;
-    const uint32_t c0 = counts[g], c1 = g + 1 < ng ? counts[g + 1] : (uint32_t)state[1];
-    const int32_t t0 = state[0], applied = state[2];
-    if (c1 == c0 || (int32_t)c0 >= applied) return;   // block-uniform
-    const uint32_t id = g * kGroupIds + threadIdx.x;
-    const uint32_t word = id < n ? bits[id >> 5] : 0u;   // the bitmap holds ceil(n/32) words
-    bool bit;
-    const uint32_t r = c0 + group_bit_rank(word, bit);
-    const int32_t fi = t0 - 1 - (int32_t)r;
-    // free-list state uploaded by a caller may be inconsistent: never index outside the pool
-    if (bit && id < n && (int32_t)r < applied && fi >= 0 && (uint32_t)fi < M) {
-        const uint32_t slot = free_list[fi];
-        if (slot < M) pool[slot] = staging[id];
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Diffuse ADVECT (shaders.js:858-997).  Kills set alive = 0 and a bit per
-// slot; k_diffuse_kill_push then pushes killed slots in ascending slot order
-// (the order a one-at-a-time kill_particle, shaders.js:914-918, produces).
+// slot; k_freelist_pass (mode 1) then pushes killed slots in ascending slot
+// order (the order a one-at-a-time kill_particle, shaders.js:914-918, produces).
 // ---------------------------------------------------------------------------
 // vel4 (binned engine): the same velocities as float4, one 16-byte load per cell.
 __device__ __forceinline__ f3 sample_grid_velocity(const float* __restrict__ mvf, const float4* __restrict__ vel4,
@@ -686,22 +594,173 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect_dev(mpm_diffuse_par
     diffuse_advect(pool, nullptr, vel4, *P, *adv, *W, kill_bits, counts);
 }
 
-// Killed slots in ascending order go to free_list[top], free_list[top+1], ...
-// One block per group of kGroupIds slots (counts: exclusive group offsets,
-// state[1] the total); groups without kills return at once.
-__global__ void __launch_bounds__(kGroupIds) k_kill_push(const uint32_t* __restrict__ bits, uint32_t M,
-                                                         const uint32_t* __restrict__ counts,
-                                                         const int32_t* __restrict__ state,
-                                                         uint32_t* __restrict__ free_list) {
-    const uint32_t g = blockIdx.x, ng = (M + kGroupIds - 1) / kGroupIds;
-    const uint32_t c0 = counts[g], c1 = g + 1 < ng ? counts[g + 1] : (uint32_t)state[1];
-    if (c1 == c0) return;   // block-uniform
-    const uint32_t i = g * kGroupIds + threadIdx.x;
-    const uint32_t word = i < M ? bits[i >> 5] : 0u;   // the bitmap holds ceil(M/32) words
-    bool bit;
-    const uint32_t r = c0 + group_bit_rank(word, bit);
-    const int32_t fi = state[0] + (int32_t)r;
-    if (bit && i < M && fi >= 0 && (uint32_t)fi < M) free_list[fi] = i;
+// One free-list pass in a single launch: the exclusive scan of the group
+// counts and the ordered pops or pushes of the free-list stack
+// (shaders.js:789-798 try_spawn, shaders.js:914-918 kill_particle), taken one
+// at a time in ascending id order.  Mode 0 (spawn): the spawner of rank r
+// takes free_list[top-1-r] while r < min(total, top).  Mode 1 (kill): the
+// killed slot of rank r goes to free_list[top+r].  Block b owns the
+// contiguous groups [b*R, (b+1)*R); every block reads all counts (a few KB)
+// for its prefix and the total, so no block waits on another.  One warp per
+// group: the group's 8 bitmap words are taken in ascending order, lane l
+// holding bit l of the word.  state = {top before, total, applied, ticket}:
+// the last block to finish (ticket) writes the new top and resets the ticket.
+constexpr int kPassThreads = 512;
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+__global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_t* __restrict__ bits, uint32_t nbits,
+                                                                const uint32_t* __restrict__ counts, uint32_t ng,
+                                                                uint32_t R, int32_t* __restrict__ top,
+                                                                int32_t* __restrict__ state,
+                                                                uint32_t* __restrict__ free_list,
+                                                                const mpm_diffuse_particle* __restrict__ staging,
+                                                                mpm_diffuse_particle* __restrict__ pool, uint32_t M,
+                                                                int mode) {
+    constexpr int kWarps = kPassThreads / 32;
+    __shared__ uint32_t red[2][kWarps];
+    __shared__ uint32_t excl[kPassThreads];
+    __shared__ int32_t s_t0;
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const uint32_t g0 = blockIdx.x * R, g1 = min(ng, g0 + R);
+    if (threadIdx.x == 0) s_t0 = *top;
+    // the total and the count before this block's first group
+    uint32_t all = 0, before = 0;
+    {
+        const uint32_t n4 = ng / 4;   // counts is 16-byte aligned (a device allocation)
+        const uint4* c4 = reinterpret_cast<const uint4*>(counts);
+        for (uint32_t i = threadIdx.x; i < n4; i += kPassThreads) {
+            const uint4 c = c4[i];
+            const uint32_t g = 4 * i;
+            all += c.x + c.y + c.z + c.w;
+            before += (g < g0 ? c.x : 0u) + (g + 1 < g0 ? c.y : 0u) + (g + 2 < g0 ? c.z : 0u) + (g + 3 < g0 ? c.w : 0u);
+        }
+        for (uint32_t g = 4 * n4 + threadIdx.x; g < ng; g += kPassThreads) {
+            const uint32_t c = counts[g];
+            all += c;
+            if (g < g0) before += c;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        all += __shfl_xor_sync(0xffffffffu, all, o);
+        before += __shfl_xor_sync(0xffffffffu, before, o);
+    }
+    if (lane == 0) { red[0][wid] = all; red[1][wid] = before; }
+    __syncthreads();
+    all = 0;
+    before = 0;
+    for (int k = 0; k < kWarps; ++k) { all += red[0][k]; before += red[1][k]; }
+    const int32_t t0 = s_t0, total = (int32_t)all;
+    const int32_t applied = mode == 0 ? (t0 > 0 ? (total < t0 ? total : t0) : 0) : total;
+    const uint32_t nwords = (nbits + 31u) / 32u;
+    uint32_t carry = before;
+    for (uint32_t base = g0; base < g1; base += kPassThreads) {
+        // exclusive scan of this tile's group counts
+        const uint32_t g = base + threadIdx.x;
+        const uint32_t c = g < g1 ? counts[g] : 0u;
+        uint32_t x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        __syncthreads();   // red is free again
+        if (lane == 31) red[0][wid] = x;
+        __syncthreads();
+        uint32_t wpre = 0;
+        for (uint32_t k = 0; k < wid; ++k) wpre += red[0][k];
+        excl[threadIdx.x] = carry + wpre + x - c;
+        uint32_t tile_total = 0;
+        for (int k = 0; k < kWarps; ++k) tile_total += red[0][k];
+        __syncthreads();
+        // one warp per group with members
+        const uint32_t tn = min(g1 - base, (uint32_t)kPassThreads);
+        for (uint32_t t = wid; t < tn; t += kWarps) {
+            const uint32_t gg = base + t;
+            const uint32_t r0 = excl[t];
+            const uint32_t cnt = (t + 1 < tn ? excl[t + 1] : carry + tile_total) - r0;
+            if (cnt == 0) continue;                                    // warp-uniform
+            if (mode == 0 && (int32_t)r0 >= applied) continue;         // no slot left for this group
+            const uint32_t wi = gg * (kGroupIds / 32) + (lane & 7u);
+            const uint32_t myword = lane < 8u && wi < nwords ? bits[wi] : 0u;
+            // lane l takes bit l of each of the 8 words; every load and store of
+            // the group is independent of the others, so all are in flight at once
+            uint32_t r = r0;
+            uint32_t slot[kGroupIds / 32];
+#pragma unroll
+            for (uint32_t j = 0; j < kGroupIds / 32; ++j) {
+                const uint32_t word = __shfl_sync(0xffffffffu, myword, j);
+                const bool bit = (word >> lane) & 1u;
+                const uint32_t rr = r + __popc(word & ((1u << lane) - 1u));
+                const uint32_t id = gg * kGroupIds + j * 32u + lane;
+                slot[j] = kNoSlot;
+                if (bit && id < nbits) {
+                    if (mode == 0) {
+                        const int32_t fi = t0 - 1 - (int32_t)rr;
+                        // free-list state uploaded by a caller may be inconsistent: never index outside the pool
+                        if ((int32_t)rr < applied && fi >= 0 && (uint32_t)fi < M) slot[j] = free_list[fi];
+                    } else {
+                        const int32_t fi = t0 + (int32_t)rr;
+                        if (fi >= 0 && (uint32_t)fi < M) free_list[fi] = id;
+                    }
+                }
+                r += __popc(word);
+            }
+            if (mode == 0) {
+                // 48-byte records as three 16-byte words (device allocations and
+                // 48-byte strides keep every record 16-byte aligned); kBatch records'
+                // loads are issued before their stores
+                constexpr uint32_t kBatch = 2;
+                static_assert(sizeof(mpm_diffuse_particle) == 48, "three 16-byte words per record");
+#pragma unroll
+                for (uint32_t jb = 0; jb < kGroupIds / 32; jb += kBatch) {
+                    uint4 rec[kBatch][3];
+#pragma unroll
+                    for (uint32_t q = 0; q < kBatch; ++q) {
+                        if (slot[jb + q] < M) {
+                            const uint4* src =
+                                reinterpret_cast<const uint4*>(staging + gg * kGroupIds + (jb + q) * 32u + lane);
+                            rec[q][0] = src[0];
+                            rec[q][1] = src[1];
+                            rec[q][2] = src[2];
+                        }
+                    }
+#pragma unroll
+                    for (uint32_t q = 0; q < kBatch; ++q) {
+                        if (slot[jb + q] < M) {
+                            uint4* dst = reinterpret_cast<uint4*>(pool + slot[jb + q]);
+                            dst[0] = rec[q][0];
+                            dst[1] = rec[q][1];
+                            dst[2] = rec[q][2];
+                        }
+                    }
+                }
+            }
+        }
+        carry += tile_total;
+        __syncthreads();   // excl is rewritten by the next tile
+    }
+    // the last block to finish publishes the new top
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t done = atomicAdd(reinterpret_cast<uint32_t*>(&state[3]), 1u);
+        if (done == gridDim.x - 1) {
+            *top = mode == 0 ? t0 - applied : t0 + total;
+            state[0] = t0;
+            state[1] = total;
+            state[2] = applied;
+            state[3] = 0;
+        }
+    }
+}
+
+// Blocks of one free-list pass over ng groups: about one group per warp, at
+// most two blocks per SM's worth.
+static inline void freelist_grid(uint32_t ng, uint32_t& B, uint32_t& R) {
+    constexpr uint32_t kWarps = kPassThreads / 32, kMaxBlocks = 2 * 148;
+    B = std::max(1u, std::min(blocks_for(ng, kWarps), kMaxBlocks));
+    R = std::max(1u, blocks_for(ng, B));
+    B = std::max(1u, blocks_for(ng, R));
 }
 
 cudaError_t launch_apply_hand(Scene& s) {
@@ -719,7 +778,6 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
     const mpm_params& P = s.params;
     DiffuseState& d = s.diffuse;
     const uint32_t n = P.particle_num;
-    const uint32_t nwords = (n + 31u) / 32u;
     const uint32_t ng = blocks_for(n, kGroupIds);
     if (n > 0) {
         Phase ph(s, MPM_PHASE_DIFFUSE_GEN);
@@ -732,10 +790,11 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
             s.launches++;
         }
         // (the binned engine's G2P has already counted the spawners per group)
-        k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, ng, d.top, d.rank_state, 0);
-        k_spawn_write<<<ng, kGroupIds, 0, st>>>(d.spawn_bits, n, d.block_counts, d.rank_state, d.free_list,
-                                                d.staging, d.pool, d.max_count);
-        s.launches += 2;
+        uint32_t B, R;
+        freelist_grid(ng, B, R);
+        k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.spawn_bits, n, d.block_counts, ng, R, d.top, d.rank_state,
+                                                    d.free_list, d.staging, d.pool, d.max_count, 0);
+        s.launches += 1;
     } else if (eval) {
         d.seed = d.seed + 1u;
     }
@@ -751,9 +810,11 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
         else
             k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, s.vel4, P, adv, s.walls, d.kill_bits,
                                                       d.block_counts);
-        k_rank_scan<<<1, 1024, 0, st>>>(d.block_counts, mg, d.top, d.rank_state, 1);
-        k_kill_push<<<mg, kGroupIds, 0, st>>>(d.kill_bits, M, d.block_counts, d.rank_state, d.free_list);
-        s.launches += 3;
+        uint32_t B, R;
+        freelist_grid(mg, B, R);
+        k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.kill_bits, M, d.block_counts, mg, R, d.top, d.rank_state,
+                                                    d.free_list, nullptr, d.pool, M, 1);
+        s.launches += 2;
     }
     return cudaGetLastError();
 }
