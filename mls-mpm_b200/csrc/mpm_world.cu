@@ -220,6 +220,14 @@ __global__ void k_count(WorldView v) {
         if (c != kHole) v.rank[i] = atomicAdd(&v.cell_count[c], 1u);
     }
 }
+// k_count for the positions [p0, p1) of a scene just imported behind counted
+// ones: their ranks continue the counts G2P left for the next binning.
+__global__ void k_count_range(WorldView v, uint32_t p0, uint32_t p1) {
+    for (uint32_t i = p0 + blockIdx.x * blockDim.x + threadIdx.x; i < p1; i += gridDim.x * blockDim.x) {
+        const uint32_t c = v.key[i];
+        if (c != kHole) v.rank[i] = atomicAdd(&v.cell_count[c], 1u);
+    }
+}
 
 // Occupied-tile list for the binning and the occupancy used by the scans.
 // tile_flags bits: 0 occupied (set by G2P / import), 1 stencil now (set by the
@@ -1869,7 +1877,6 @@ cudaError_t world_add_scene(World& w, uint32_t X, uint32_t Y, uint32_t Z, const 
     r.id_base = (uint32_t)ib; r.n = n; r.id_cap = n ? n : 1;
     world_set_uniforms(w, slot, P, W, nullptr, 0, nullptr);
     w.generation++;
-    w.counted = false;
     for (uint32_t t = 0; t < nt; ++t) w.h_tile_scene[tb + t] = (uint32_t)slot;
     e = cudaMemcpyAsync(w.tile_scene + tb, w.h_tile_scene.data() + tb, (size_t)nt * 4, cudaMemcpyHostToDevice,
                         w.stream);
@@ -1882,6 +1889,13 @@ cudaError_t world_add_scene(World& w, uint32_t X, uint32_t Y, uint32_t Z, const 
                                                      w.posm[w.cur], w.velid[w.cur], w.aff[w.cur], n);
         k_set_total<<<1, 1, 0, w.stream>>>(w.ctrl, h_total + n);
         w.launches += 3;
+        // the other positions keep the ranks G2P counted: count only the new
+        // ones (before any count, the next substep counts everything)
+        if (w.counted) {
+            k_count_range<<<std::min<uint32_t>(cdiv(n, 256), w.pos_blocks), 256, 0, w.stream>>>(v, h_total,
+                                                                                             h_total + n);
+            w.launches++;
+        }
         e = cudaGetLastError();
         w.pos_bound = h_total + n;
     }
@@ -1917,6 +1931,9 @@ cudaError_t world_remove_scene(World& w, int slot) {
     if (e == cudaSuccess) e = cudaMemsetAsync(w.mvf + 3ull * r.cell_base, 0, (size_t)r.G * 12, w.stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.vel4 + r.cell_base, 0, (size_t)r.G * 16, w.stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.tile_flags + r.tile_base, 0, (size_t)r.ntiles * 4, w.stream);
+    // the counts G2P left in the scene's cells: the other scenes' counts and
+    // ranks stay valid, so no recount is needed
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.cell_count + r.cell_base, 0, (size_t)r.G * 4, w.stream);
     for (uint32_t t = 0; t < r.ntiles; ++t) w.h_tile_scene[r.tile_base + t] = kHole;
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(w.tile_scene + r.tile_base, w.h_tile_scene.data() + r.tile_base, (size_t)r.ntiles * 4,
@@ -1933,7 +1950,6 @@ cudaError_t world_remove_scene(World& w, int slot) {
     r = SceneRec();
     w.table_dirty = true;
     w.generation++;
-    w.counted = false;
     if (e == cudaSuccess) e = cudaGetLastError();
     return e;
 }
@@ -1978,7 +1994,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
         e = cudaMemsetAsync(w.ctrl, 0, kCtrlZeroBytes, st);
         if (e != cudaSuccess) return e;
         if (!w.counted) {
-            // scenes were added or removed since the last G2P counted: recount
+            // nothing counted yet (a new world, or positions edited in place): count all
             e = cudaMemsetAsync(w.cell_count, 0, ((size_t)w.cell_cap + 1) * 4, st);
             if (e != cudaSuccess) return e;
             k_count<<<nposb, 256, 0, st>>>(v);
