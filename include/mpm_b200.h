@@ -140,7 +140,8 @@ mpm_status mpm_diffuse_set_gen_params(mpm_scene* scene, const mpm_gen_params* ge
  * each.  Enqueues work and returns. */
 mpm_status mpm_step(mpm_scene* scene, int substeps);
 
-/* Wait for all work enqueued on the scene's stream. */
+/* Wait for all work enqueued on the scene's stream, and for queued
+ * alive-count readbacks. */
 mpm_status mpm_sync(mpm_scene* scene);
 
 /* Device pointer and byte size of a buffer in its reference layout (valid
@@ -172,10 +173,12 @@ mpm_status mpm_upload(mpm_scene* scene, mpm_buffer which, const void* host_src, 
 mpm_status mpm_diffuse_alive_count(mpm_scene* scene, int32_t* alive);
 
 /* DiffuseGPU.requestDebugReadback (diffuse-gpu.js:172-176), asynchronous: a
- * 4-byte copy of freeListTop queued on the scene stream after the work
- * already enqueued, into a ring of 4 pinned slots.  With every slot still in
- * flight it first waits for the oldest one (so the host never runs more than
- * 4 readbacks ahead of the device). */
+ * 4-byte copy of freeListTop as of the work already enqueued, into a ring of
+ * 4 pinned slots.  With every slot still in flight it first waits for the
+ * oldest one (so the host never runs more than 4 readbacks ahead of the
+ * device).  After a step the copy reads the value the last kill pass recorded
+ * on the device and runs on a side stream, so later steps do not wait for it;
+ * after top was uploaded or exported it copies top itself, in stream order. */
 mpm_status mpm_diffuse_request_alive(mpm_scene* scene);
 
 /* DiffuseGPU.pollDebug (diffuse-gpu.js:178-188), non-blocking: reads every

@@ -113,6 +113,7 @@ static void free_scene(Scene& s) {
     void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
                     s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
                     s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.rank_state, s.diffuse.staging,
+                    s.diffuse.top_hist,
                     s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word, s.diffuse.gen_dev,
                     s.diffuse.adv_dev};
     for (void* p : ptrs)
@@ -121,6 +122,8 @@ static void free_scene(Scene& s) {
     if (s.diffuse.alive_ring) cudaFreeHost(s.diffuse.alive_ring);
     for (cudaEvent_t& ev : s.diffuse.alive_ev)
         if (ev) cudaEventDestroy(ev);
+    if (s.diffuse.rb_after) cudaEventDestroy(s.diffuse.rb_after);
+    if (s.diffuse.rb_stream) cudaStreamDestroy(s.diffuse.rb_stream);
     if (s.edit_host) cudaFreeHost(s.edit_host);
     if (s.stream) cudaStreamDestroy(s.stream);
 }
@@ -194,8 +197,27 @@ static cudaError_t import_state(Scene& s) {
     return e;
 }
 
+// A readback still copying from top_hist must finish before the kill pass
+// kTopHist passes later overwrites its entry: the scene stream waits for it.
+static cudaError_t guard_top_history(Scene& s) {
+    DiffuseState& d = s.diffuse;
+    if (!d.enabled) return cudaSuccess;
+    constexpr uint32_t R = DiffuseState::kAliveRing;
+    for (uint32_t i = d.alive_tail; i != d.alive_head; ++i) {
+        const uint32_t t = i % R;
+        if (d.alive_pass[t] != UINT64_MAX && d.alive_pass[t] + DiffuseState::kTopHist <= d.passes) {
+            const cudaError_t e = cudaStreamWaitEvent(s.stream, d.alive_ev[t], 0);
+            if (e != cudaSuccess) return e;
+            d.alive_pass[t] = UINT64_MAX;
+        }
+    }
+    return cudaSuccess;
+}
+
 static cudaError_t launch_substep(Scene& s) {
     s.substeps_done++;
+    const cudaError_t ge = guard_top_history(s);
+    if (ge != cudaSuccess) return ge;
     if (s.engine == kEnginePlain) return launch_substep_plain(s);
     s.ref_stale = true;
     world_set_uniforms(s.world, s.world_slot, s.params, s.walls, &s.hand, s.hand_active, s.hand_dims);
@@ -429,7 +451,10 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     if (e == cudaSuccess) e = dalloc(&d.spawn_bits, nwN * 4);
     if (e == cudaSuccess) e = dalloc(&d.kill_bits, nwM * 4);
     if (e == cudaSuccess) e = dalloc(&d.block_counts, nb * 4);
-    if (e == cudaSuccess) e = dalloc(&d.rank_state, 16);
+    if (e == cudaSuccess) e = dalloc(&d.rank_state, 32);
+    if (e == cudaSuccess) e = dalloc(&d.top_hist, DiffuseState::kTopHist * 4);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d.rb_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d.rb_after, cudaEventDisableTiming);
     if (e == cudaSuccess) e = dalloc(&d.staging, N * 48);
     if (e == cudaSuccess) e = dalloc(&d.gen_dev, sizeof(mpm_gen_params));
     if (e == cudaSuccess) e = dalloc(&d.adv_dev, sizeof(mpm_advect_params));
@@ -445,7 +470,7 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     CUDA_TRY(cudaMemcpyAsync(d.free_list, fl.data(), M * 4, cudaMemcpyHostToDevice, s.stream), "free list");
     CUDA_TRY(cudaMemcpyAsync(d.top, &top, 4, cudaMemcpyHostToDevice, s.stream), "top");
     CUDA_TRY(cudaMemsetAsync(d.pool, 0, M * 48, s.stream), "pool");
-    CUDA_TRY(cudaMemsetAsync(d.rank_state, 0, 16, s.stream), "free-list pass state");
+    CUDA_TRY(cudaMemsetAsync(d.rank_state, 0, 32, s.stream), "free-list pass state");
     CUDA_TRY(cudaStreamSynchronize(s.stream), "diffuse init sync");
     d.max_count = (uint32_t)M;
     d.gen = *gen;
@@ -491,12 +516,15 @@ mpm_status mpm_sync(mpm_scene* sc) {
     if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     DeviceGuard guard(sc->s.device);
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "mpm_sync");
+    // queued alive-count readbacks have landed too
+    if (sc->s.diffuse.rb_stream) CUDA_TRY(cudaStreamSynchronize(sc->s.diffuse.rb_stream), "mpm_sync readbacks");
     return MPM_OK;
 }
 
 mpm_status mpm_get_buffer(mpm_scene* sc, mpm_buffer which, void** dev_ptr, size_t* bytes) {
     if (!sc || !dev_ptr || !bytes) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     if (!buffer_info(sc->s, which, dev_ptr, bytes)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
+    if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_exported = true;
     if (is_particle_buffer(which)) {
         DeviceGuard guard(sc->s.device);
         CUDA_TRY(sync_reference_buffers(sc->s), "export");
@@ -525,6 +553,7 @@ mpm_status mpm_get_ipc_handle(mpm_scene* sc, mpm_buffer which, void* handle, siz
     void* p;
     size_t sz;
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
+    if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_exported = true;
     DeviceGuard guard(sc->s.device);
     if (is_particle_buffer(which)) CUDA_TRY(sync_reference_buffers(sc->s), "export");
     CUdeviceptr base = 0;
@@ -557,6 +586,7 @@ mpm_status mpm_upload(mpm_scene* sc, mpm_buffer which, const void* host_src, siz
     void* p;
     size_t sz;
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
+    if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_written = true;
     if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
     DeviceGuard guard(sc->s.device);
     if (is_particle_buffer(which)) {
@@ -592,8 +622,23 @@ mpm_status mpm_diffuse_request_alive(mpm_scene* sc) {
         ++d.alive_tail;
     }
     const uint32_t h = d.alive_head % R;
-    CUDA_TRY(cudaMemcpyAsync(d.alive_ring + h, d.top, 4, cudaMemcpyDeviceToHost, sc->s.stream), "alive readback");
-    CUDA_TRY(cudaEventRecord(d.alive_ev[h], sc->s.stream), "alive readback event");
+    if (d.passes == 0 || d.top_written || d.top_exported) {
+        // top may differ from the last kill pass's: copy it in stream order
+        CUDA_TRY(cudaMemcpyAsync(d.alive_ring + h, d.top, 4, cudaMemcpyDeviceToHost, sc->s.stream), "alive readback");
+        CUDA_TRY(cudaEventRecord(d.alive_ev[h], sc->s.stream), "alive readback event");
+        d.alive_pass[h] = UINT64_MAX;
+    } else {
+        // top is what the latest kill pass left in top_hist: copy that entry on
+        // the side stream once the scene stream gets here, without holding the
+        // scene stream back
+        const uint64_t k = d.passes - 1;
+        CUDA_TRY(cudaEventRecord(d.rb_after, sc->s.stream), "alive readback point");
+        CUDA_TRY(cudaStreamWaitEvent(d.rb_stream, d.rb_after, 0), "alive readback order");
+        CUDA_TRY(cudaMemcpyAsync(d.alive_ring + h, d.top_hist + k % DiffuseState::kTopHist, 4, cudaMemcpyDeviceToHost,
+                                 d.rb_stream), "alive readback");
+        CUDA_TRY(cudaEventRecord(d.alive_ev[h], d.rb_stream), "alive readback event");
+        d.alive_pass[h] = k;
+    }
     ++d.alive_head;
     return MPM_OK;
 }

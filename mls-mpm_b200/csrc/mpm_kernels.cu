@@ -604,7 +604,8 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect_dev(mpm_diffuse_par
 // for its prefix and the total, so no block waits on another.  One warp per
 // group: the group's 8 bitmap words are taken in ascending order, lane l
 // holding bit l of the word.  state = {top before, total, applied, ticket}:
-// the last block to finish (ticket) writes the new top and resets the ticket.
+// the last block to finish (ticket) writes the new top and resets the ticket;
+// a kill pass also appends the new top to top_hist (state[4] counts them).
 constexpr int kPassThreads = 512;
 constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
 __global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_t* __restrict__ bits, uint32_t nbits,
@@ -614,7 +615,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_
                                                                 uint32_t* __restrict__ free_list,
                                                                 const mpm_diffuse_particle* __restrict__ staging,
                                                                 mpm_diffuse_particle* __restrict__ pool, uint32_t M,
-                                                                int mode) {
+                                                                int mode, int32_t* __restrict__ top_hist) {
     constexpr int kWarps = kPassThreads / 32;
     __shared__ uint32_t red[2][kWarps];
     __shared__ uint32_t excl[kPassThreads];
@@ -745,11 +746,17 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_
         __threadfence();
         const uint32_t done = atomicAdd(reinterpret_cast<uint32_t*>(&state[3]), 1u);
         if (done == gridDim.x - 1) {
-            *top = mode == 0 ? t0 - applied : t0 + total;
+            const int32_t nt = mode == 0 ? t0 - applied : t0 + total;
+            *top = nt;
             state[0] = t0;
             state[1] = total;
             state[2] = applied;
             state[3] = 0;
+            if (mode == 1) {   // kill pass k leaves the substep's final top in top_hist[k % kTopHist]
+                const uint32_t k = (uint32_t)state[4];
+                top_hist[k % DiffuseState::kTopHist] = nt;
+                state[4] = (int32_t)(k + 1u);
+            }
         }
     }
 }
@@ -793,7 +800,7 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
         uint32_t B, R;
         freelist_grid(ng, B, R);
         k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.spawn_bits, n, d.block_counts, ng, R, d.top, d.rank_state,
-                                                    d.free_list, d.staging, d.pool, d.max_count, 0);
+                                                    d.free_list, d.staging, d.pool, d.max_count, 0, nullptr);
         s.launches += 1;
     } else if (eval) {
         d.seed = d.seed + 1u;
@@ -813,8 +820,10 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
         uint32_t B, R;
         freelist_grid(mg, B, R);
         k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.kill_bits, M, d.block_counts, mg, R, d.top, d.rank_state,
-                                                    d.free_list, nullptr, d.pool, M, 1);
+                                                    d.free_list, nullptr, d.pool, M, 1, d.top_hist);
         s.launches += 2;
+        d.passes++;
+        d.top_written = false;
     }
     return cudaGetLastError();
 }

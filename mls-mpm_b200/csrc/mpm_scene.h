@@ -30,7 +30,7 @@ struct DiffuseState {
     uint32_t* spawn_bits = nullptr;         // ceil(N/32) words, one bit per fluid particle id
     uint32_t* kill_bits = nullptr;          // ceil(M/32) words, one bit per slot
     uint32_t* block_counts = nullptr;       // max(ceil(N/8192), ceil(M/8192)) + 1
-    int32_t* rank_state = nullptr;          // [0] = top before the pass, [1] = total, [2] = applied
+    int32_t* rank_state = nullptr;          // [0] top before the pass, [1] total, [2] applied, [3] ticket, [4] kill passes
     mpm_diffuse_particle* staging = nullptr;  // N x 48 B spawn records indexed by particle id
     int32_t* host_top = nullptr;            // pinned 4 B for alive-count readback
     // asynchronous alive-count readbacks (requestDebugReadback / pollDebug):
@@ -40,6 +40,16 @@ struct DiffuseState {
     cudaEvent_t alive_ev[kAliveRing] = {};
     uint32_t alive_head = 0, alive_tail = 0;   // next slot to fill / oldest unread
     int32_t alive_last = 0;                 // latest value read back
+    uint64_t alive_pass[kAliveRing] = {};   // kill pass whose top each slot reads
+    // top after each kill pass, kept on the device so a readback copies it on
+    // a side stream and the scene stream never waits for that copy
+    static constexpr uint32_t kTopHist = 256;
+    int32_t* top_hist = nullptr;            // kTopHist entries, written by the kill pass
+    uint64_t passes = 0;                    // kill passes enqueued (host mirror of rank_state[4])
+    bool top_written = false;               // top changed outside a kill pass since the last one
+    bool top_exported = false;              // a caller holds top's device address
+    cudaStream_t rb_stream = nullptr;       // readback side stream
+    cudaEvent_t rb_after = nullptr;         // scene-stream point a readback copies after
     mpm_gen_params* gen_dev = nullptr;      // device GenParams (binned engine: seed bumped on the device)
     mpm_advect_params* adv_dev = nullptr;   // device copy of adv (binned engine)
 };

@@ -2088,6 +2088,7 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
         const uint64_t l0 = w.launches;
         const uint64_t sl0 = dsc ? dsc->launches : 0;
         const uint32_t seed0 = dsc ? dsc->diffuse.seed : 0;
+        const uint64_t passes0 = dsc ? dsc->diffuse.passes : 0;
         cudaGraph_t g = nullptr;
         e = cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;
@@ -2106,6 +2107,7 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
         if (dsc) {
             dsc->launches = sl0;
             dsc->diffuse.seed = seed0;
+            dsc->diffuse.passes = passes0;
         }
         if (e != cudaSuccess) {
             w.graph[p] = nullptr;
@@ -2118,7 +2120,11 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
     if (e != cudaSuccess) return e;
     // host mirror of what the graph does
     w.launches += w.graph_kernels[p];
-    if (dsc) dsc->diffuse.seed += 1u;
+    if (dsc) {
+        dsc->diffuse.seed += 1u;
+        dsc->diffuse.passes += 1u;   // the graph's kill pass
+        dsc->diffuse.top_written = false;
+    }
     w.pos_bound = w.n_total;   // the layout after a substep is dense
     w.cm_current = w.grid_i32[w.gbuf];
     w.cur ^= 1;
