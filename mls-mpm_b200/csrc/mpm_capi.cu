@@ -112,7 +112,8 @@ static void free_scene(Scene& s) {
     }
     void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
                     s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
-                    s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.rank_state, s.diffuse.staging,
+                    s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.kill_counts, s.diffuse.rank_state,
+                    s.diffuse.staging,
                     s.diffuse.top_hist,
                     s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word, s.diffuse.gen_dev,
                     s.diffuse.adv_dev};
@@ -451,6 +452,7 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     if (e == cudaSuccess) e = dalloc(&d.spawn_bits, nwN * 4);
     if (e == cudaSuccess) e = dalloc(&d.kill_bits, nwM * 4);
     if (e == cudaSuccess) e = dalloc(&d.block_counts, nb * 4);
+    if (e == cudaSuccess) e = dalloc(&d.kill_counts, nb * 4);
     if (e == cudaSuccess) e = dalloc(&d.rank_state, 32);
     if (e == cudaSuccess) e = dalloc(&d.top_hist, DiffuseState::kTopHist * 4);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d.rb_stream, cudaStreamNonBlocking);
@@ -471,6 +473,9 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     CUDA_TRY(cudaMemcpyAsync(d.top, &top, 4, cudaMemcpyHostToDevice, s.stream), "top");
     CUDA_TRY(cudaMemsetAsync(d.pool, 0, M * 48, s.stream), "pool");
     CUDA_TRY(cudaMemsetAsync(d.rank_state, 0, 32, s.stream), "free-list pass state");
+    // the spawn bits and counts start clear; each kill pass clears them again
+    CUDA_TRY(cudaMemsetAsync(d.spawn_bits, 0, nwN * 4, s.stream), "spawn bits");
+    CUDA_TRY(cudaMemsetAsync(d.block_counts, 0, nb * 4, s.stream), "spawn counts");
     CUDA_TRY(cudaStreamSynchronize(s.stream), "diffuse init sync");
     d.max_count = (uint32_t)M;
     d.gen = *gen;

@@ -615,7 +615,10 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_
                                                                 uint32_t* __restrict__ free_list,
                                                                 const mpm_diffuse_particle* __restrict__ staging,
                                                                 mpm_diffuse_particle* __restrict__ pool, uint32_t M,
-                                                                int mode, int32_t* __restrict__ top_hist) {
+                                                                int mode, int32_t* __restrict__ top_hist,
+                                                                uint32_t* __restrict__ clear_bits, uint32_t nclear_bits,
+                                                                uint32_t* __restrict__ clear_counts,
+                                                                uint32_t nclear_counts) {
     constexpr int kWarps = kPassThreads / 32;
     __shared__ uint32_t red[2][kWarps];
     __shared__ uint32_t excl[kPassThreads];
@@ -740,6 +743,12 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_
         carry += tile_total;
         __syncthreads();   // excl is rewritten by the next tile
     }
+    // (kill pass) the spawn bits and counts were last read by the spawn pass:
+    // clear them for the next substep's G2P
+    for (uint32_t i = blockIdx.x * kPassThreads + threadIdx.x; i < nclear_bits; i += gridDim.x * kPassThreads)
+        clear_bits[i] = 0u;
+    for (uint32_t i = blockIdx.x * kPassThreads + threadIdx.x; i < nclear_counts; i += gridDim.x * kPassThreads)
+        clear_counts[i] = 0u;
     // the last block to finish publishes the new top
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -800,7 +809,8 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
         uint32_t B, R;
         freelist_grid(ng, B, R);
         k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.spawn_bits, n, d.block_counts, ng, R, d.top, d.rank_state,
-                                                    d.free_list, d.staging, d.pool, d.max_count, 0, nullptr);
+                                                    d.free_list, d.staging, d.pool, d.max_count, 0, nullptr, nullptr, 0,
+                                                    nullptr, 0);
         s.launches += 1;
     } else if (eval) {
         d.seed = d.seed + 1u;
@@ -813,14 +823,15 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
         Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
         if (P_dev && W_dev && s.vel4)
             k_diffuse_advect_dev<<<mg, kThreads, 0, st>>>(d.pool, s.vel4, P_dev, d.adv_dev, W_dev, d.kill_bits,
-                                                          d.block_counts);
+                                                          d.kill_counts);
         else
             k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, s.vel4, P, adv, s.walls, d.kill_bits,
-                                                      d.block_counts);
+                                                      d.kill_counts);
         uint32_t B, R;
         freelist_grid(mg, B, R);
-        k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.kill_bits, M, d.block_counts, mg, R, d.top, d.rank_state,
-                                                    d.free_list, nullptr, d.pool, M, 1, d.top_hist);
+        k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.kill_bits, M, d.kill_counts, mg, R, d.top, d.rank_state,
+                                                    d.free_list, nullptr, d.pool, M, 1, d.top_hist, d.spawn_bits,
+                                                    (n + 31u) / 32u, d.block_counts, ng);
         s.launches += 2;
         d.passes++;
         d.top_written = false;

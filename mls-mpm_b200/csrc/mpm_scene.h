@@ -29,7 +29,8 @@ struct DiffuseState {
     // ranking scratch
     uint32_t* spawn_bits = nullptr;         // ceil(N/32) words, one bit per fluid particle id
     uint32_t* kill_bits = nullptr;          // ceil(M/32) words, one bit per slot
-    uint32_t* block_counts = nullptr;       // max(ceil(N/8192), ceil(M/8192)) + 1
+    uint32_t* block_counts = nullptr;       // spawners per group of kGroupIds fluid ids
+    uint32_t* kill_counts = nullptr;        // kills per group of kGroupIds slots
     int32_t* rank_state = nullptr;          // [0] top before the pass, [1] total, [2] applied, [3] ticket, [4] kill passes
     mpm_diffuse_particle* staging = nullptr;  // N x 48 B spawn records indexed by particle id
     int32_t* host_top = nullptr;            // pinned 4 B for alive-count readback

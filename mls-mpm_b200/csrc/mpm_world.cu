@@ -1540,6 +1540,13 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     const float bubble_min = dv.enabled ? dv.gen->density_bubble_min : 0.0f;
     const float pressure_threshold = dv.enabled ? dv.gen->pressure_threshold : 0.0f;
     const float ke_threshold = dv.enabled ? dv.gen->ke_threshold : 0.0f;
+    // the per-substep counters of the binning and the grid passes are read
+    // no more in this substep: clear them for the next one
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        v.ctrl->n_occ = 0u;
+        v.ctrl->n_grid = 0u;
+        v.ctrl->bins_done = 0u;
+    }
     // chunk headers: the next one's words are copied while this chunk runs
     if (threadIdx.x == 0 && blockIdx.x < nch) hs = unpack_header(v.chunk_hdr[2ull * blockIdx.x], v.chunk_hdr[2ull * blockIdx.x + 1]);
     __syncthreads();
@@ -1991,8 +1998,6 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     cudaError_t e;
     {
         Phase ph(prof, MPM_PHASE_SORT);
-        e = cudaMemsetAsync(w.ctrl, 0, kCtrlZeroBytes, st);
-        if (e != cudaSuccess) return e;
         if (!w.counted) {
             // nothing counted yet (a new world, or positions edited in place): count all
             e = cudaMemsetAsync(w.cell_count, 0, ((size_t)w.cell_cap + 1) * 4, st);
@@ -2037,13 +2042,8 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
         k_update_tiles<<<w.grid_blocks, 256, 0, st>>>(v, cm, mv, w.mvf, w.vel4, cm_n, mv_n);
         w.launches++;
     }
-    if (dv.enabled) {
-        const uint32_t n = w.scenes[dv.scene].n;
-        e = cudaMemsetAsync(dv.spawn_bits, 0, ((size_t)(n + 31) / 32) * 4, st);
-        if (e != cudaSuccess) return e;
-        e = cudaMemsetAsync(dv.group_counts, 0, ((size_t)(n + kGroupIds - 1) / kGroupIds) * 4, st);
-        if (e != cudaSuccess) return e;
-    }
+    // (the spawn bits and group counts G2P adds to were cleared by the
+    // previous substep's kill pass)
     {
         Phase ph(prof, MPM_PHASE_G2P);
         k_g2p_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4, w.cmf, w.posm[nxt],

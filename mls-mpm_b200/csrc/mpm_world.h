@@ -54,8 +54,9 @@ struct alignas(16) SceneDesc {
 };
 static_assert(sizeof(SceneDesc) == 576, "bench.py SCENE_DESC_BYTES counts this block per uniform upload");
 
-// Small device-side control block.  The first kCtrlZeroBytes are cleared at
-// the start of every substep.
+// Small device-side control block.  The first kCtrlZeroBytes (per-substep
+// counters) start at zero and are cleared again by G2P, which runs after
+// their last use in the substep.
 struct Ctrl {
     uint32_t n_occ, n_grid, bins_done, pad1;   // bins_done: k_bin_cells blocks finished
     // persistent
