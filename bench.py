@@ -295,7 +295,7 @@ def main():
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": phase_ms[dom]}
-    traffic = _profile_traffic(dom)
+    traffic = _profile_traffic(dom, args.workload)
     if traffic:
         roofline["traffic"] = traffic
 
@@ -305,7 +305,7 @@ def main():
             "config": {"workload": args.workload, "grid": list(scene.grid), "particles": n,
                        "diffuse_pool": scene.diffuse_max, "substeps_per_step": 1,
                        "parallelism": f"scene-sharded x{ws}" if ws > 1 else "single scene",
-                       "l2": "working set > 126 MB L2 (particles 76 MB + grids 64 MB + pool 13 MB); no flush"},
+                       "l2": l2_note(n, G, scene.diffuse_max)},
             "roofline": roofline,
             "substep_roofline": {"achieved": sub_bytes / (sub_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                                  "frac": sub_bytes / (sub_ms * 1e-3) / 1e9 / peak,
@@ -509,6 +509,18 @@ def served_comparison(local, rates=(50.0, 200.0, 2000.0), count=64, seed=0, budg
 # kernel that carries each timed phase (for the DRAM traffic of its ncu summary)
 PHASE_KERNEL = {"p2g_mass": "k_p2g_mass_chunks", "p2g_mom": "k_p2g_mom_chunks", "g2p": "k_g2p_chunks",
                 "update_grid": "k_update_tiles"}
+
+
+def l2_note(n, cells, pool):
+    """How the timed substeps stand against the 126 MB L2: the state read and
+    written every substep (particles 72 B: position, velocity, affine,
+    density; grid cells 32 B: i32 mass and momentum, float4 velocity; diffuse
+    slots 48 B)."""
+    mb = lambda b: b / 2**20
+    p, g, d = 72 * n, 32 * cells, 48 * pool
+    rel = ">" if p + g + d > 126e6 else "<="
+    return (f"working set {rel} 126 MB L2 (particles {mb(p):.0f} MB + grids {mb(g):.0f} MB + pool {mb(d):.0f} MB); "
+            "no flush")
 
 
 def _profile_traffic(phase, workload=WORKLOAD):
