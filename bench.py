@@ -240,20 +240,7 @@ def main():
     n_launch = c1.value - c0.value
     fl.destroy()
 
-    # (2) per-phase device time over the same substeps (CUDA events on the scene stream)
-    fl = make()
-    lib, h = fl._lib, fl._scene
-    lib.mpm_profile_enable(h, 1)
-    lib.mpm_profile_read(h, None, None, 1)
-    for _ in range(args.steps):
-        check(lib.mpm_step(h, 1), "mpm_step")
-    pm = (ctypes.c_double * 10)()
-    pc = (ctypes.c_uint64 * 10)()
-    check(lib.mpm_profile_read(h, pm, pc, 1), "mpm_profile_read")
-    names = [lib.mpm_phase_name(i).decode() for i in range(10)]
-    fl.destroy()
-
-    # (3) end to end through the public API over the same substeps, as the
+    # (2) end to end through the public API over the same substeps, as the
     # reference's frame drives it (main.js:504-528): per step the host moves
     # the hand (fluid-gpu.js:479-527; a small cylinder sweeping the empty top
     # corner of the domain, so every frame carries new uniforms, uploaded from
@@ -276,6 +263,21 @@ def main():
         fl.diffuse.pollDebug()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     fl.destroy()
+
+    # (3) per-phase device time over the same substeps (CUDA events on the scene stream),
+    # after the end-to-end run so that both timed loops follow each other
+    fl = make()
+    lib, h = fl._lib, fl._scene
+    lib.mpm_profile_enable(h, 1)
+    lib.mpm_profile_read(h, None, None, 1)
+    for _ in range(args.steps):
+        check(lib.mpm_step(h, 1), "mpm_step")
+    pm = (ctypes.c_double * 10)()
+    pc = (ctypes.c_uint64 * 10)()
+    check(lib.mpm_profile_read(h, pm, pc, 1), "mpm_profile_read")
+    names = [lib.mpm_phase_name(i).decode() for i in range(10)]
+    fl.destroy()
+
     h2d = SCENE_DESC_BYTES   # the scene's uniform block, changed by the hand every frame
     d2h = 4 if scene.diffuse_max else 0
 
