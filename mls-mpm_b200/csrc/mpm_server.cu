@@ -35,7 +35,8 @@ using Clock = std::chrono::steady_clock;
 
 struct Job {
     mpm_params P{};
-    std::vector<float> pos, vel, mass;
+    std::vector<float> pos, vel, mass;   // page-locked while the job waits (pinned = true)
+    bool pinned = false;
     uint32_t n = 0, substeps = 0, left = 0;
     double arrival = 0.0, admit = -1.0;
     volatile double finish = -1.0;   // written by the stream-ordered host function
@@ -53,6 +54,40 @@ void CUDART_CB stamp_finish(void* p) {
 mpm_status sfail(mpm_status st, const std::string& msg) {
     mpm::set_error(msg);
     return st;
+}
+
+// A job's input arrays are page-locked when it is submitted, so its upload at
+// admission is an asynchronous copy: the serving loop never blocks on it
+// while the device runs out of queued substeps.  Without page-locking the
+// upload still works, as a copy from pageable memory.
+void pin_inputs(Job& j) {
+    bool ok = true;
+    for (std::vector<float>* v : {&j.pos, &j.vel, &j.mass}) {
+        if (v->empty()) continue;
+        if (cudaHostRegister(v->data(), v->size() * sizeof(float), cudaHostRegisterDefault) != cudaSuccess) {
+            cudaGetLastError();   // clear the error: the pageable path still works
+            ok = false;
+        }
+    }
+    if (ok) {
+        j.pinned = true;
+        return;
+    }
+    for (std::vector<float>* v : {&j.pos, &j.vel, &j.mass})
+        if (!v->empty() && cudaHostUnregister(v->data()) != cudaSuccess) cudaGetLastError();
+}
+
+// Release the inputs of an admitted job (only once no copy from them can be
+// in flight: after a stream synchronisation).
+void release_inputs(Job& j) {
+    if (j.pinned) {
+        for (std::vector<float>* v : {&j.pos, &j.vel, &j.mass})
+            if (!v->empty()) cudaHostUnregister(v->data());
+        j.pinned = false;
+    }
+    std::vector<float>().swap(j.pos);
+    std::vector<float>().swap(j.vel);
+    std::vector<float>().swap(j.mass);
 }
 
 double percentile(std::vector<double> v, double q) {
@@ -127,7 +162,8 @@ mpm_status mpm_server_create(const mpm_server_desc* d, mpm_server** out) {
 
 mpm_status mpm_server_destroy(mpm_server* s) {
     if (!s) return MPM_OK;
-    mpm_batch_destroy(s->batch);
+    mpm_batch_destroy(s->batch);   // waits for the batch's stream
+    for (auto& j : s->jobs) release_inputs(*j);
     delete s;
     return MPM_OK;
 }
@@ -149,6 +185,13 @@ mpm_status mpm_server_submit(mpm_server* s, const mpm_params* P, const float* po
     j->pos.assign(pos4, pos4 + (size_t)n * 4);
     if (vel4) j->vel.assign(vel4, vel4 + (size_t)n * 4);
     j->mass.assign(mass, mass + n);
+    {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(s->device);
+        pin_inputs(*j);
+        if (prev >= 0) cudaSetDevice(prev);
+    }
     j->t0 = &s->t0;
     *job = (int64_t)s->jobs.size();
     s->jobs.push_back(std::move(j));
@@ -206,10 +249,7 @@ mpm_status mpm_server_run(mpm_server* s, mpm_server_stats* stats) {
             if (st != MPM_OK) return st;   // an empty batch that cannot take the job never will
             j->sid = sid;
             j->admit = t;
-            j->state = 1;
-            std::vector<float>().swap(j->pos);
-            std::vector<float>().swap(j->vel);
-            std::vector<float>().swap(j->mass);
+            j->state = 1;   // its inputs are released after the final synchronisation
             queue.pop_front();
             active.push_back(j);
         }
@@ -256,6 +296,8 @@ mpm_status mpm_server_run(mpm_server* s, mpm_server_stats* stats) {
         active.resize(w);
     }
     if (cudaStreamSynchronize(stream) != cudaSuccess) return sfail(MPM_ERR_DEVICE, "final sync");
+    for (Job* j : this_run)
+        if (j->state != 0) release_inputs(*j);
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
         std::vector<double> lat;
