@@ -396,8 +396,10 @@ mpm_status mpm_server_create(const mpm_server_desc* desc, mpm_server** out);
 mpm_status mpm_server_destroy(mpm_server* server);
 
 /* Queues a job.  params: grid dims and uniforms as mpm_set_params takes them
- * (particle_num replaced by n); host arrays are copied.  MPM_ERR_CAPACITY if
- * the job can never fit the server. */
+ * (particle_num replaced by n); host arrays are copied into page-locked host
+ * memory (pageable if page-locking fails), held until the mpm_server_run
+ * that admits the job returns, so admission uploads are asynchronous.
+ * MPM_ERR_CAPACITY if the job can never fit the server. */
 mpm_status mpm_server_submit(mpm_server* server, const mpm_params* params, const float* pos4, const float* vel4,
                              const float* mass, uint32_t n, uint32_t substeps, double arrival_s, int64_t* job);
 
