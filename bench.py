@@ -300,6 +300,12 @@ def main():
     traffic = _profile_traffic(dom, args.workload)
     if traffic:
         roofline["traffic"] = traffic
+    # the same kernel's issue-slot use (sm__inst_issued, ncu): what bounds it
+    issue = _profile_value("issue_active_per_launch", dom, args.workload)
+    if issue is not None:
+        roofline["issue_active"] = issue
+        roofline["issue_note"] = ("fraction of issue slots used, from the committed ncu summary: the particle "
+                                  "kernels are issue/latency-bound, not HBM-bound")
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sub_ms, "higher_is_better": True, "scaling": "weak",
@@ -525,10 +531,9 @@ def l2_note(n, cells, pool):
             "no flush")
 
 
-def _profile_traffic(phase, workload=WORKLOAD):
-    """DRAM bytes (read + write) per launch of the phase's kernel, from the
-    `dram_bytes_per_launch <kernel> <workload> <bytes>` lines of the committed
-    ncu summaries under profiles/, or None."""
+def _profile_value(key, phase, workload):
+    """The value of a `<key> <kernel> <workload> <value>` line of the committed
+    ncu summaries under profiles/ for the phase's kernel, or None."""
     kernel = PHASE_KERNEL.get(phase)
     d = os.path.join(ROOT, "profiles")
     if not kernel or not os.path.isdir(d):
@@ -538,9 +543,16 @@ def _profile_traffic(phase, workload=WORKLOAD):
             continue
         for line in open(os.path.join(d, f)):
             parts = line.split()
-            if len(parts) == 4 and parts[0] == "dram_bytes_per_launch" and parts[1] == kernel and parts[2] == workload:
-                return int(parts[3])
+            if len(parts) == 4 and parts[0] == key and parts[1] == kernel and parts[2] == workload:
+                return float(parts[3])
     return None
+
+
+def _profile_traffic(phase, workload=WORKLOAD):
+    """DRAM bytes (read + write) per launch of the phase's kernel, from the
+    `dram_bytes_per_launch <kernel> <workload> <bytes>` lines, or None."""
+    v = _profile_value("dram_bytes_per_launch", phase, workload)
+    return int(v) if v is not None else None
 
 
 if __name__ == "__main__":
