@@ -605,7 +605,9 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect_dev(mpm_diffuse_par
 // group: the group's 8 bitmap words are taken in ascending order, lane l
 // holding bit l of the word.  state = {top before, total, applied, ticket}:
 // the last block to finish (ticket) writes the new top and resets the ticket;
-// a kill pass also appends the new top to top_hist (state[4] counts them).
+// a kill pass also appends the new top to top_hist (state[4] counts them) and
+// clears the spawn bits and counts (clear_bits, clear_counts) that the spawn
+// pass before it read, ready for the next substep's G2P.
 constexpr int kPassThreads = 512;
 constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
 __global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_t* __restrict__ bits, uint32_t nbits,
