@@ -74,7 +74,33 @@ struct mpm_batch {
     uint32_t flags = 0;
     uint64_t substeps = 0;
     Tuner tune;
+    // device staging of an added scene's reference-layout arrays, kept
+    // between adds and grown to the largest scene.  Allocating it per add
+    // (stream-ordered pool) blocked the host for up to 0.16 s while the pool
+    // re-mapped memory, and freeing an outgrown buffer (cudaFree) for up to
+    // 0.45 s next to a large world, so outgrown buffers are kept until the
+    // batch is destroyed.
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
+    std::vector<void*> stage_old;
 };
+
+namespace mpm {
+// Staging for a scene of n particles (72 bytes each), allocated before it is
+// needed (the serving loop reserves for its largest job before it starts).
+cudaError_t batch_reserve_stage(mpm_batch* b, uint32_t n) {
+    const size_t need = (size_t)(n ? n : 1) * 72;
+    if (need <= b->stage_bytes) return cudaSuccess;
+    const size_t bytes = std::max(need, (size_t)64 << 20);
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return e;
+    if (b->stage) b->stage_old.push_back(b->stage);   // a queued import may still read it
+    b->stage = p;
+    b->stage_bytes = bytes;
+    return cudaSuccess;
+}
+}  // namespace mpm
 
 namespace {
 
@@ -185,7 +211,9 @@ mpm_status mpm_batch_destroy(mpm_batch* b) {
     if (!b) return MPM_OK;
     DevGuard g(b->device);
     cudaStream_t st = b->w.stream;
-    world_free(b->w);
+    world_free(b->w);   // waits for the stream
+    if (b->stage) cudaFree(b->stage);
+    for (void* p : b->stage_old) cudaFree(p);
     for (cudaEvent_t& e : b->tune.ev)
         if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
@@ -214,14 +242,15 @@ mpm_status mpm_batch_add(mpm_batch* b, const mpm_params* P, const mpm_wall_param
     if (G > w.cell_cap) return bfail(MPM_ERR_CAPACITY, "grid larger than the batch's cell capacity");
     DevGuard g(b->device);
     cudaStream_t st = w.stream;
-    // stage the host arrays in the reference layouts on the device
-    float4 *dpos = nullptr, *dvel = nullptr;
-    float *daff = nullptr, *dmass = nullptr;
+    // stage the host arrays in the reference layouts on the device (pos 16,
+    // vel 16, affine 36, mass 4 bytes per particle; the last add's import
+    // reads it earlier in stream order)
     const size_t N = n ? n : 1;
-    BATCH_TRY(cudaMallocAsync((void**)&dpos, N * 16, st), "stage pos");
-    BATCH_TRY(cudaMallocAsync((void**)&dvel, N * 16, st), "stage vel");
-    BATCH_TRY(cudaMallocAsync((void**)&daff, N * 36, st), "stage affine");
-    BATCH_TRY(cudaMallocAsync((void**)&dmass, N * 4, st), "stage mass");
+    BATCH_TRY(batch_reserve_stage(b, n), "stage allocation");
+    float4* dpos = reinterpret_cast<float4*>(b->stage);
+    float4* dvel = dpos + N;
+    float* daff = reinterpret_cast<float*>(dvel + N);
+    float* dmass = daff + 9 * N;
     cudaError_t e = cudaSuccess;
     if (n) {
         e = cudaMemcpyAsync(dpos, pos4, (size_t)n * 16, cudaMemcpyHostToDevice, st);
@@ -238,10 +267,6 @@ mpm_status mpm_batch_add(mpm_batch* b, const mpm_params* P, const mpm_wall_param
     int slot = -1;
     if (e == cudaSuccess)
         e = world_add_scene(w, P->grid_X, P->grid_Y, P->grid_Z, *P, W ? *W : none, dpos, dvel, daff, dmass, n, &slot);
-    cudaFreeAsync(dpos, st);
-    cudaFreeAsync(dvel, st);
-    cudaFreeAsync(daff, st);
-    cudaFreeAsync(dmass, st);
     if (e == cudaErrorMemoryAllocation) return bfail(MPM_ERR_CAPACITY, "no free cell, tile or id range for the scene");
     if (e == cudaErrorNotReady) return bfail(MPM_ERR_BUSY, "particle layout full; step once, then add");
     BATCH_TRY(e, "mpm_batch_add");

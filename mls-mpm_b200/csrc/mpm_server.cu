@@ -27,6 +27,9 @@
 
 namespace mpm {
 void set_error(const std::string& msg);
+// Device staging of a batch (mpm_batch.cu) large enough to add a scene of n
+// particles without allocating then.
+cudaError_t batch_reserve_stage(mpm_batch* b, uint32_t n);
 }
 
 namespace {
@@ -231,6 +234,12 @@ mpm_status mpm_server_run(mpm_server* s, mpm_server_stats* stats) {
     } events{ev};
     mpm_batch_info i0;
     mpm_batch_get_info(s->batch, &i0);
+    // staging for the largest queued job, allocated before the clock starts
+    {
+        uint32_t nmax = 0;
+        for (const Job* j : queue) nmax = std::max(nmax, j->n);
+        if (mpm::batch_reserve_stage(s->batch, nmax) != cudaSuccess) return sfail(MPM_ERR_OOM, "staging allocation");
+    }
     std::vector<Job*> active;
     uint64_t k = 0, updates = 0, active_sum = 0, active_max = 0;
     const bool keep = (s->flags & MPM_SERVER_KEEP_STATE) != 0;
