@@ -325,7 +325,10 @@ mpm_status mpm_batch_destroy(mpm_batch* batch);
  * may be NULL (none), host particle arrays as mpm_upload_particles takes
  * them.  *scene receives the scene id.  MPM_ERR_CAPACITY when particles,
  * cells or scene slots are exhausted; MPM_ERR_BUSY when the particle layout
- * still holds removed scenes' slots (step once, then add). */
+ * still holds removed scenes' slots (step once, then add).  The arrays are
+ * copied in stream order (asynchronously from page-locked memory) through a
+ * device staging buffer the batch keeps and grows to its largest scene
+ * (72 B per particle; outgrown buffers are released by mpm_batch_destroy). */
 mpm_status mpm_batch_add(mpm_batch* batch, const mpm_params* params, const mpm_wall_params* walls,
                          const float* pos4, const float* vel4, const float* affine9, const float* mass, uint32_t n,
                          int32_t* scene);
