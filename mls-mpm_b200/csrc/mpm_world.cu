@@ -5,7 +5,8 @@
 //   * Particles are sorted by (tile, cell) every substep (counting sort: the
 //     rank of each particle in its new cell is taken in G2P, then a scan per
 //     16x8x8-cell tile and a two-level scan over tiles) and each tile's
-//     particles are cut into chunks of up to kChunk consecutive particles.
+//     particles are cut into chunks of up to kChunk consecutive particles
+//     (kChunkSmall in worlds too small to fill the chunk kernels' grid).
 //     The new layout reads the previous one through a permutation (new
 //     position -> previous position), which stays nearly coalesced because
 //     the order changes little between substeps.
@@ -97,6 +98,7 @@ WorldView World::view() const {
     v.ngroups = (v.ntiles + 1023u) / 1024u;
     if (v.ngroups == 0) v.ngroups = 1;
     v.chunk_cap = chunk_cap;
+    v.chunk = chunk;
     v.scenes = d_scenes;
     v.tile_scene = tile_scene;
     v.cell_count = cell_count; v.cell_start = cell_start;
@@ -376,7 +378,7 @@ __global__ void __launch_bounds__(1024) k_tile_scan_local(WorldView v) {
     const uint32_t g = blockIdx.x;
     const uint32_t t = g * 1024u + threadIdx.x;
     const uint32_t np = (t < v.ntiles && v.tile_occ[t]) ? v.tile_cnt[t] : 0u;
-    const uint32_t nc = (np + kChunk - 1) / kChunk;
+    const uint32_t nc = (np + v.chunk - 1) / v.chunk;
     uint32_t tp, tc;
     const uint32_t rp = block_exclusive_scan_1024(np, ws, tp);
     const uint32_t rc = block_exclusive_scan_1024(nc, ws, tc);
@@ -434,7 +436,7 @@ __device__ void tiles_fold(const WorldView& v, mpm_gen_params* gen) {
         const uint32_t t = t0 + threadIdx.x;
         // tile counts written by the other blocks of k_bin_cells: read past L1
         const uint32_t np = (t < v.ntiles && v.tile_occ[t]) ? __ldcg(v.tile_cnt + t) : 0u;
-        const uint32_t nc = (np + kChunk - 1) / kChunk;
+        const uint32_t nc = (np + v.chunk - 1) / v.chunk;
         uint32_t tp, tc;
         const uint32_t rp = block_exclusive_scan_1024(np, ws, tp);
         const uint32_t rc = block_exclusive_scan_1024(nc, ws, tc);
@@ -482,11 +484,12 @@ __global__ void __launch_bounds__(kTileCells) k_tile_finish(WorldView v) {
         const uint32_t a = v.cell_start[c];
         v.cell_start[c] = base_p + a;
         v.cell_count[c] = 0u;
-        for (uint32_t j = a / kChunk; j <= (a + cnt - 1) / kChunk; ++j) {
+        const uint32_t C = v.chunk;
+        for (uint32_t j = a / C; j <= (a + cnt - 1) / C; ++j) {
             const uint32_t ci = base_c + j;
             if (ci >= v.chunk_cap) break;
-            const uint32_t f = j * kChunk;
-            const uint32_t e = min(f + kChunk, total);
+            const uint32_t f = j * C;
+            const uint32_t e = min(f + C, total);
             if (f >= a) {
                 v.chunk_info[ci] = make_uint4(t, base_p + f, base_p + e, lid);
                 v.chunk_geo[ci] = make_uint4(scene, tx, ty, tz);
@@ -691,9 +694,10 @@ __device__ __forceinline__ void mass_contrib_shared(const PW& w, float m, int32_
 // ---------------------------------------------------------------------------
 // P2G_MASS (shaders.js:242-274): one block per chunk, one thread per particle
 // ---------------------------------------------------------------------------
+template <uint32_t kC>
 __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, const float4* __restrict__ posm,
                                                                    int32_t* __restrict__ cm) {
-    constexpr int kPer = kChunk / kChunkThreads;
+    constexpr int kPer = kC / kChunkThreads;
     __shared__ int32_t acc[kHaloCells];
     const uint32_t nch = v.ctrl->total_chunks;
     __shared__ ChunkHdr hs;
@@ -1157,13 +1161,14 @@ __device__ __forceinline__ void mom_load(const WorldView& v, uint32_t p, bool va
     for (int e = 0; e < 9; ++e) a[e] = valid ? aff[e * plane + slot] : 0.0f;
 }
 
+template <uint32_t kC>
 __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(WorldView v, const float4* __restrict__ posm,
                                                                    const float4* __restrict__ velid,
                                                                    const float* __restrict__ aff,
                                                                    const float* __restrict__ cmf,
                                                                    int32_t* __restrict__ mv,
                                                                    float* __restrict__ dens) {
-    constexpr int kPer = kChunk / kChunkThreads;
+    constexpr int kPer = kC / kChunkThreads;
     __shared__ float mh[2][kHaloCells];
     __shared__ int32_t acc[3][kHaloCells];
     __shared__ ChunkHdr hdr[2];
@@ -1522,6 +1527,7 @@ __device__ __noinline__ void g2p_direct_particle(const G2POut o, const SceneDesc
     o.rank[p] = g2p_store(o, sd, p, q, vi, o.dens[p], r.gv[0], r.gv[1], r.gv[2], r.B);
 }
 
+template <uint32_t kC>
 __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(WorldView v, const float4* __restrict__ posm,
                                                               const float4* __restrict__ velid,
                                                               const float4* __restrict__ vel4,
@@ -1529,7 +1535,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
                                                               float4* __restrict__ posm_out,
                                                               float4* __restrict__ velid_out,
                                                               float* __restrict__ aff_out, DiffuseView dv) {
-    constexpr int kPer = kChunk / kChunkThreads;
+    constexpr int kPer = kC / kChunkThreads;
     __shared__ float4 vh[kHaloCells];   // staged grid velocities (x, y, z, 0)
     __shared__ uint4 nhs[2];              // the next chunk's header words
     const uint32_t nch = v.ctrl->total_chunks;
@@ -1662,7 +1668,7 @@ static void world_plan(World& w, uint32_t particle_cap, uint64_t cell_cap, uint3
     w.id_cap = particle_cap;
     w.scene_cap = scene_cap;
     // every occupied tile has at most one partial chunk
-    w.chunk_cap = w.npos / kChunk + w.tile_cap + 1;
+    w.chunk_cap = w.npos / kChunkSmall + w.tile_cap + 1;   // room for the smaller chunks
 }
 
 // Every device array of a world with its size (one list for allocation,
@@ -2025,7 +2031,10 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     }
     {
         Phase ph(prof, MPM_PHASE_P2G_MASS);
-        k_p2g_mass_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], cm);
+        if (w.chunk == kChunkSmall)
+            k_p2g_mass_chunks<kChunkSmall><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], cm);
+        else
+            k_p2g_mass_chunks<kChunk><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], cm);
         w.launches++;
     }
     {
@@ -2035,8 +2044,12 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     }
     {
         Phase ph(prof, MPM_PHASE_P2G_MOM);
-        k_p2g_mom_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.aff[cur], w.cmf, mv,
-                                                                w.dens);
+        if (w.chunk == kChunkSmall)
+            k_p2g_mom_chunks<kChunkSmall><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur],
+                                                                                 w.aff[cur], w.cmf, mv, w.dens);
+        else
+            k_p2g_mom_chunks<kChunk><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur],
+                                                                            w.aff[cur], w.cmf, mv, w.dens);
         w.launches++;
     }
     {
@@ -2048,8 +2061,14 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
     // previous substep's kill pass)
     {
         Phase ph(prof, MPM_PHASE_G2P);
-        k_g2p_chunks<<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4, w.cmf, w.posm[nxt],
-                                                            w.velid[nxt], w.aff[nxt], dv);
+        if (w.chunk == kChunkSmall)
+            k_g2p_chunks<kChunkSmall><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4,
+                                                                             w.cmf, w.posm[nxt], w.velid[nxt],
+                                                                             w.aff[nxt], dv);
+        else
+            k_g2p_chunks<kChunk><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4,
+                                                                        w.cmf, w.posm[nxt], w.velid[nxt],
+                                                                        w.aff[nxt], dv);
         w.launches++;
     }
     w.cur = nxt;
@@ -2069,6 +2088,13 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
 }
 
 cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
+    // chunk size: one pass per chunk when full-size chunks would leave blocks
+    // of the chunk kernels idle (a new size means new captured graphs)
+    const uint32_t chunk = (uint64_t)w.n_total < (uint64_t)w.item_blocks * kChunk ? kChunkSmall : kChunk;
+    if (chunk != w.chunk) {
+        w.chunk = chunk;
+        w.generation++;
+    }
     cudaError_t e = world_upload_table(w);
     if (e != cudaSuccess) return e;
     const bool diffuse = ds && ds->diffuse.enabled;

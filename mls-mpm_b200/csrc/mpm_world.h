@@ -34,6 +34,11 @@ constexpr int kTileCells = kTileX * kTileY * kTileZ;   // 1024: one thread per c
 constexpr uint32_t kChunk = MPM_CHUNK;
 constexpr int kChunkThreads = MPM_CHUNK_THREADS;
 static_assert(kChunk % kChunkThreads == 0, "a chunk is a whole number of passes of the block");
+// Small worlds, whose kChunk-particle chunks would not fill the chunk
+// kernels' grid, are cut into chunks of one pass instead (shorter blocks on
+// more SMs); the size is chosen per substep.
+constexpr uint32_t kChunkSmall = kChunkThreads;
+static_assert(kChunkSmall <= kChunk, "the small chunk is one pass");
 // Largest halo box (a whole tile plus one cell on every side).
 constexpr int kHaloCells = (kTileX + 2) * (kTileY + 2) * (kTileZ + 2);
 // Positions of the layout beyond the particle count: none (the layout is
@@ -73,6 +78,7 @@ struct WorldView {
     uint32_t ntiles;           // tiles in use (end of the allocated tile range)
     uint32_t ngroups;          // ceil(ntiles / 1024): groups of the two-level tile scan
     uint32_t chunk_cap;        // capacity of the chunk list
+    uint32_t chunk;            // particles per chunk this substep (kChunk or kChunkSmall)
     const SceneDesc* scenes;
     const uint32_t* tile_scene;    // scene of each global tile (kHole: free)
     uint32_t* cell_count;      // total cells + 1, zero outside binning
@@ -184,6 +190,7 @@ struct World {
     uint4* chunk_hdr = nullptr;
     uint4* chunk_geo = nullptr;
     uint32_t chunk_cap = 0;
+    uint32_t chunk = kChunk;   // chunk size of the substep being enqueued
     uint32_t* tile_occ_list = nullptr;
     uint32_t* tile_grid_list = nullptr;
     Ctrl* ctrl = nullptr;
