@@ -169,3 +169,34 @@ def test_batch_capacity_errors(gpu):
         assert b.info().particles == 9100
     finally:
         b.close()
+
+
+def test_chunk_size_switch_between_substeps(gpu):
+    """A world that grows past the size where 512-particle chunks fill the
+    chunk kernels' grid (about 300k particles on 148 SMs) switches from
+    one-pass to full-size chunks between substeps, and back after a removal;
+    every scene stays bit-exact against the oracle through both switches."""
+    a = S.crowded()
+    big = S.Scenario("big", scenes.small_box(grid=(96, 64, 96), n=400_000, seed=5, name="big"), 6)
+    fa, fb = script(a, 12), script(big, 6)
+    b = new_batch(particles=600_000, cells=1_500_000)
+    try:
+        ia = b.add_scene(a.scene, fa[0][0])
+        for t in range(3):                      # a small world: one-pass chunks
+            set_uniforms(b, ia, *fa[t])
+            b.step(1)
+        ib = b.add_scene(big.scene, fb[0][0])   # past the threshold: full-size chunks
+        for t in range(3, 9):
+            set_uniforms(b, ia, *fa[t])
+            set_uniforms(b, ib, *fb[t - 3])
+            b.step(1)
+        got_b = read_all(b, ib)
+        b.remove(ib)                            # small again
+        for t in range(9, 12):
+            set_uniforms(b, ia, *fa[t])
+            b.step(1)
+        got_a = read_all(b, ia)
+    finally:
+        b.close()
+    assert diff_report(oracle_states(a, fa, (12,))[12], got_a) == []
+    assert diff_report(oracle_states(big, fb, (6,))[6], got_b) == []
