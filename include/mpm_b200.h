@@ -327,8 +327,8 @@ mpm_status mpm_batch_destroy(mpm_batch* batch);
  * cells or scene slots are exhausted; MPM_ERR_BUSY when the particle layout
  * still holds removed scenes' slots (step once, then add).  The arrays are
  * copied in stream order through a device staging buffer the batch keeps and
- * grows to its largest scene (72 B per particle; outgrown buffers are
- * released by mpm_batch_destroy).  From page-locked memory the copy is
+ * grows to its largest scene (76 B per particle, shared with particle
+ * downloads; outgrown buffers are released by mpm_batch_destroy).  From page-locked memory the copy is
  * asynchronous: keep such arrays unchanged until the batch's stream has
  * passed the add (any later mpm_batch_download, or a stream synchronize). */
 mpm_status mpm_batch_add(mpm_batch* batch, const mpm_params* params, const mpm_wall_params* walls,

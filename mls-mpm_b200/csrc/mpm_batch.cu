@@ -86,10 +86,11 @@ struct mpm_batch {
 };
 
 namespace mpm {
-// Staging for a scene of n particles (72 bytes each), allocated before it is
-// needed (the serving loop reserves for its largest job before it starts).
+// Staging for a scene of n particles (76 bytes each: an add uses 72, a
+// particle download 76), allocated before it is needed (the serving loop
+// reserves for its largest job before it starts).
 cudaError_t batch_reserve_stage(mpm_batch* b, uint32_t n) {
-    const size_t need = (size_t)(n ? n : 1) * 72;
+    const size_t need = (size_t)(n ? n : 1) * 76;
     if (need <= b->stage_bytes) return cudaSuccess;
     const size_t bytes = std::max(need, (size_t)64 << 20);
     void* p = nullptr;
@@ -348,7 +349,6 @@ mpm_status mpm_batch_download(mpm_batch* b, int32_t scene, mpm_buffer which, voi
     const size_t n = r.n, G = r.G;
     size_t size = 0;
     const void* src = nullptr;
-    void* staging = nullptr;
     int32_t *cm, *mv;
     float *cmf, *mvf;
     world_scene_grid(w, scene, &cm, &mv, &cmf, &mvf);
@@ -358,9 +358,11 @@ mpm_status mpm_batch_download(mpm_batch* b, int32_t scene, mpm_buffer which, voi
         case MPM_BUF_CELL_MASS_F32: src = cmf; size = G * 4; break;
         case MPM_BUF_CELL_MV_F32: src = mvf; size = G * 12; break;
         case MPM_BUF_POS: case MPM_BUF_VEL: case MPM_BUF_AFFINE: case MPM_BUF_MASS: case MPM_BUF_DENSITY: {
+            // the batch's staging buffer (queued imports read it earlier in
+            // stream order; this download waits for its copy before returning)
             const size_t N = n ? n : 1;
-            BATCH_TRY(cudaMallocAsync(&staging, N * (16 + 16 + 36 + 4 + 4), st), "download staging");
-            char* base = (char*)staging;
+            BATCH_TRY(batch_reserve_stage(b, (uint32_t)n), "download staging");
+            char* base = (char*)b->stage;
             float4* pos = (float4*)base;
             float4* vel = (float4*)(base + N * 16);
             float* aff = (float*)(base + N * 32);
@@ -368,10 +370,7 @@ mpm_status mpm_batch_download(mpm_batch* b, int32_t scene, mpm_buffer which, voi
             float* dens = (float*)(base + N * 72);
             cudaError_t e = cudaMemsetAsync(dens, 0, N * 4, st);
             if (e == cudaSuccess) e = world_export_scene(w, scene, pos, vel, aff, mass, dens);
-            if (e != cudaSuccess) {
-                cudaFreeAsync(staging, st);
-                return bcuda(e, "export");
-            }
+            if (e != cudaSuccess) return bcuda(e, "export");
             if (which == MPM_BUF_POS) { src = pos; size = n * 16; }
             if (which == MPM_BUF_VEL) { src = vel; size = n * 16; }
             if (which == MPM_BUF_AFFINE) { src = aff; size = n * 36; }
@@ -383,7 +382,6 @@ mpm_status mpm_batch_download(mpm_batch* b, int32_t scene, mpm_buffer which, voi
     }
     cudaError_t e = bytes > size ? cudaErrorInvalidValue : cudaSuccess;
     if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, st);
-    if (staging) cudaFreeAsync(staging, st);
     if (e == cudaErrorInvalidValue) return bfail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
     BATCH_TRY(e, "download");
     BATCH_TRY(cudaStreamSynchronize(st), "download sync");
