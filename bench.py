@@ -138,23 +138,30 @@ def cpu_reference_rate(scene, substeps, threads, budget_s=None, warmup=1):
     return scene.n * done / dt, kind, done, dt
 
 
+def run_config(workload, scene, ws):
+    """The `config` object of both arms' lines."""
+    return {"workload": workload, "grid": list(scene.grid), "particles": scene.n,
+            "diffuse_pool": scene.diffuse_max, "substeps_per_step": 1,
+            "parallelism": f"scene-sharded x{ws}" if ws > 1 else "single scene",
+            "l2": l2_note(scene.n, scene.cells, scene.diffuse_max)}
+
+
 def run_reference_arm(args, ws, rank):
     from mls_mpm_b200 import scenes
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    scene = scenes.dam_break_1m(0)
+    scene = scenes.WORKLOADS[args.workload](seed=0)
     # warm-up steps are untimed; each timed step is one full substep of the
     # scene; the run is capped at ~240 s of CPU time (the sample is stated)
     rate, kind, done, secs = cpu_reference_rate(scene, args.steps, threads, budget_s=240.0, warmup=args.warmup)
-    sample = f"{done} substeps of the {WORKLOAD} scene (1,048,576 particles + 262,144 diffuse pool) " \
-             f"on {threads} host threads"
+    sample = f"{done} substeps of the {args.workload} scene ({scene.n:,} particles + {scene.diffuse_max:,} " \
+             f"diffuse pool) on {threads} host threads"
     line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
             "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+i32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD, "grid": [128, 128, 128], "particles": 1048576,
-                       "diffuse_pool": 262144, "substeps_per_step": 1},
+            "config": run_config(args.workload, scene, ws),
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -310,10 +317,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sub_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+i32", "data": "synthetic",
-            "config": {"workload": args.workload, "grid": list(scene.grid), "particles": n,
-                       "diffuse_pool": scene.diffuse_max, "substeps_per_step": 1,
-                       "parallelism": f"scene-sharded x{ws}" if ws > 1 else "single scene",
-                       "l2": l2_note(n, G, scene.diffuse_max)},
+            "config": run_config(args.workload, scene, ws),
             "roofline": roofline,
             "substep_roofline": {"achieved": sub_bytes / (sub_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                                  "frac": sub_bytes / (sub_ms * 1e-3) / 1e9 / peak,
