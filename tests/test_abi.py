@@ -89,3 +89,13 @@ def test_batch_footprint_without_device(native):
     # ~150 B per particle (two state copies + layout) + ~56 B per cell (two i32 grids + decoded grid)
     assert 140 * (1 << 20) + 50 * (1 << 21) < out[0] < 200 * (1 << 20) + 80 * (1 << 21)
     assert out[0] < out[1] < out[2]
+
+
+def test_noalloc_source_calls_no_allocator():
+    """mpm_compact_noalloc's source names no device allocator or pool call
+    (comments aside), so the entry point cannot allocate on any path."""
+    src = open(os.path.join(ROOT, "mls-mpm_b200", "csrc", "mpm_noalloc.cu")).read()
+    code = re.sub(r"//[^\n]*", "", re.sub(r"/\*.*?\*/", "", src, flags=re.S))
+    banned = re.findall(r"\b(cudaMalloc\w*|cudaFree\w*|cudaMemPool\w*|cuMem\w*|malloc|free|new\s|"
+                        r"cudaHostAlloc|cudaMallocHost|c10|torch)\b", code)
+    assert not banned, banned

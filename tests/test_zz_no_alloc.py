@@ -1,8 +1,12 @@
 """mpm_compact_noalloc against mpm_compact: same survivors, counts and order
 on two calls in a row with different inputs (the second call must not see
-the first call's scratch), no device memory taken by a call after the first,
-and the size limit rejected on the host.  Collected last so it also runs
-after every other GPU test in the same process."""
+the first call's scratch); no allocation from the device's default memory
+pool during a call, where mpm_compact's stream-ordered scratch shows up (so
+the check can see an allocation); n = 0, NULL arguments and the size limit
+rejected or handled on the host.  mpm_compact_noalloc is for callers that
+must not allocate device memory while they run: a frame loop with a fixed
+memory plan, or a host whose allocator belongs to someone else.  Collected
+last so it also runs after every other GPU test in the same process."""
 import ctypes
 
 import numpy as np
@@ -39,6 +43,37 @@ def _outputs(tensors):
     return cnt, torch.full_like(tp, -7.0), torch.full_like(tv, -7.0), torch.full_like(tm, -7.0)
 
 
+class _PoolHighWater:
+    """High-water mark of the device's default memory pool (where
+    cudaMallocAsync takes stream-ordered memory), through the driver API."""
+
+    def __init__(self, ordinal=0):
+        from cuda.bindings import driver
+        self.d = driver
+        err, = driver.cuInit(0)
+        assert err == driver.CUresult.CUDA_SUCCESS, err
+        err, dev = driver.cuDeviceGet(ordinal)
+        assert err == driver.CUresult.CUDA_SUCCESS, err
+        err, self.pool = driver.cuDeviceGetDefaultMemPool(dev)
+        assert err == driver.CUresult.CUDA_SUCCESS, err
+
+    def _attr(self, name):
+        err, v = self.d.cuMemPoolGetAttribute(self.pool, getattr(self.d.CUmemPool_attribute, name))
+        assert err == self.d.CUresult.CUDA_SUCCESS, err
+        return int(v)
+
+    def reset(self):
+        """Restart the high-water mark at the bytes in use now; returns them."""
+        zero = self.d.cuuint64_t(0)
+        err, = self.d.cuMemPoolSetAttribute(self.pool, self.d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH,
+                                           zero)
+        assert err == self.d.CUresult.CUDA_SUCCESS, err
+        return self._attr("CU_MEMPOOL_ATTR_USED_MEM_CURRENT")
+
+    def high(self):
+        return self._attr("CU_MEMPOOL_ATTR_USED_MEM_HIGH")
+
+
 def _run(lib, fn, ray, tensors, n, stream, outs=None):
     tp, tv, tm = tensors
     cnt, op, ov, om = outs if outs is not None else _outputs(tensors)
@@ -54,17 +89,21 @@ def test_noalloc_compact_matches_mpm_compact_two_calls_in_a_row(gpu):
     stream = torch.cuda.current_stream().cuda_stream
     cases = [(300_001, _ray((24.0, 24.0, 24.0), (1.0, 0.5, 0.2), 9.0)),   # drops a thick cylinder
              (70_000, _ray((5.0, 40.0, 10.0), (0.0, 0.0, 1.0), 2.0))]     # fewer particles, thin cylinder
-    free_after = []
+    pool = _PoolHighWater(0)
     for n, ray in cases:
         tensors = tuple(torch.from_numpy(a).to(dev) for a in _inputs(rng, n))
         outs = _outputs(tensors)
         torch.cuda.synchronize()
-        free_before = torch.cuda.mem_get_info(dev)[0]
+        in_use = pool.reset()
         got = _run(gpu, "mpm_compact_noalloc", ray, tensors, n, stream, outs)
         torch.cuda.synchronize()
-        free_after.append((free_before, torch.cuda.mem_get_info(dev)[0]))
+        # nothing was taken from the pool during the call
+        assert pool.high() == in_use
+        in_use = pool.reset()
         want = _run(gpu, "mpm_compact", ray, tensors, n, stream)
         torch.cuda.synchronize()
+        # the allocating entry point does show up: the check can see an allocation
+        assert pool.high() > in_use
         m = int(want[0].item())
         assert int(got[0].item()) == m
         assert 0 < m < n
@@ -72,9 +111,39 @@ def test_noalloc_compact_matches_mpm_compact_two_calls_in_a_row(gpu):
             assert torch.equal(g[:m].view(torch.int32), w[:m].view(torch.int32))
             # nothing past the survivors is written
             assert bool((g[m:] == -7.0).all())
-    # calls after the first one on this device take no device memory
-    before, after = free_after[1]
-    assert after == before
+
+
+def test_noalloc_compact_empty_input_sets_count_only(gpu):
+    """n = 0: *count_dev becomes 0 and no output is touched."""
+    import torch
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(11)
+    tensors = tuple(torch.from_numpy(a).to(dev) for a in _inputs(rng, 8))
+    outs = _outputs(tensors)
+    ray = _ray((1.0, 1.0, 1.0), (0.0, 1.0, 0.0), 3.0)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        cnt, op, ov, om = _run(gpu, "mpm_compact_noalloc", ray, tensors, 0, stream, outs)
+        torch.cuda.synchronize()
+        assert int(cnt.item()) == 0
+        for o in (op, ov, om):
+            assert bool((o == -7.0).all())
+        cnt.fill_(99)
+
+
+def test_noalloc_compact_null_arguments_rejected(gpu):
+    import torch
+    dev = torch.device("cuda:0")
+    t = torch.zeros((4, 4), dtype=torch.float32, device=dev)
+    cnt = torch.zeros((1,), dtype=torch.int32, device=dev)
+    ray = _ray((0.0, 0.0, 0.0), (1.0, 0.0, 0.0), 1.0)
+    p = t.data_ptr()
+    stream = torch.cuda.current_stream().cuda_stream
+    # NULL ray, NULL count, NULL input with n > 0: MPM_ERR_INVALID_ARG, nothing enqueued
+    assert gpu.mpm_compact_noalloc(None, 4, p, p, p, p, p, p, cnt.data_ptr(), stream) == 1
+    assert gpu.mpm_compact_noalloc(ctypes.byref(ray), 4, p, p, p, p, p, p, None, stream) == 1
+    assert gpu.mpm_compact_noalloc(ctypes.byref(ray), 4, None, p, p, p, p, p, cnt.data_ptr(), stream) == 1
+    assert b"NULL" in gpu.mpm_last_error()
 
 
 def test_noalloc_compact_rejects_oversize_on_the_host(gpu):
