@@ -18,16 +18,17 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "lib", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmpm_ref.so")
-REF_SOURCE = "/root/reference"
 
 _libs = {}
 
 
 def build_oracle():
-    """Compile the oracle (and the reference pin when the reference is present)."""
+    """Compile the oracle, and the reference pin when the reference checkout is
+    present.  Where the checkout lies is the recipe's business: environment
+    variable MPM_REFERENCE_DIR, else the Makefile's default; the recipe skips
+    the pin when that directory holds no shaders.js."""
     subprocess.run(["make", "-s", "-C", HERE, "lib/liboracle.so"], check=True)
-    if os.path.isdir(REF_SOURCE):
-        subprocess.run(["make", "-s", "-C", HERE, "_ref/libmpm_ref.so", f"REF_DIR={REF_SOURCE}"], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
 
 
 def _load(path, build=True):
@@ -81,9 +82,7 @@ def to_f64(st):
     for k, v in st.items():
         out[k] = v.astype(np.float64) if v.dtype == np.float32 else v.copy()
     if "diffuse" in st:
-        d = st["diffuse"]
-        f = np.zeros((d.shape[0], 6), np.float64)
-        out["diffuse"] = d.copy()   # f64 diffuse is not tracked
+        out["diffuse"] = st["diffuse"].copy()   # f64 diffuse is not tracked
     return out
 
 

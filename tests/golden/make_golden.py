@@ -7,7 +7,9 @@ the host in dispatch order.  For every scenario in tests/scenarios.py this
 records the SHA-256 of each state array after every substep, plus a few
 summary numbers.  Run it where the reference checkout exists:
 
-    python tests/golden/make_golden.py            # needs /root/reference
+    MPM_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py
+
+(without MPM_REFERENCE_DIR, oracle/Makefile's default location is used).
 
 The GPU box has no reference checkout; the committed JSON carries the pin there.
 """
@@ -35,7 +37,9 @@ def main():
     for name, make in scenarios.SCENARIOS.items():
         sc = make()
         steps = []
-        for s, (ref, orc) in enumerate(zip(cpu_run(sc, "ref"), cpu_run(sc, "oracle"))):
+        # the pin one thread wide: its diffuse free-list pops are in particle
+        # order only then (the canonical order the oracle and the GPU keep)
+        for s, (ref, orc) in enumerate(zip(cpu_run(sc, "ref", threads=1), cpu_run(sc, "oracle", threads=8))):
             bad = diff_report(ref, orc)
             if bad:
                 raise SystemExit(f"oracle != reference pin in {name} substep {s}: {bad}")
