@@ -79,7 +79,8 @@ def walls_hand_diffuse():
     return Scenario("walls_hand_diffuse", sc, 40, diffuse_max=500, walls=_walls_moving, hand=_hand_sweep)
 
 
-def dam_break_64(substeps=20):
+def dam_break_64(substeps=200):
+    """The 64^3 configuration (65,536 particles) over its full 200 substeps."""
     return Scenario("dam_break_64", scenes.dam_break_64(0), substeps)
 
 

@@ -12,8 +12,9 @@ pytestmark = pytest.mark.gpu
 
 
 def _scenario(substeps):
-    # the C2 grid with a dam block and a falling sphere, 8 particles per cell
-    # over a quarter of the width: ~0.5M particles
+    # the 256x128x256 grid with a dam block only (no sphere), 8 particles per
+    # cell in a 24 x 48-cell footprint: 524,288 particles.  The full 8M-particle
+    # configuration with its falling sphere is in test_gpu_configs.py.
     n = 1 << 19
     nx, ny = 48, 96
     nz = -(-n // (nx * ny))

@@ -20,7 +20,7 @@ def test_oracle_matches_golden(name):
     sc = scenarios.SCENARIOS[name]()
     gold = GOLDEN["scenarios"][name]
     assert gold["n"] == sc.scene.n and gold["substeps"] == sc.substeps
-    for s, st in enumerate(cpu_run(sc, "oracle")):
+    for s, st in enumerate(cpu_run(sc, "oracle", threads=4)):
         d = O.digest(st)
         bad = [k for k, v in gold["steps"][s]["digest"].items() if d.get(k) != v]
         assert not bad, f"{name} substep {s}: {bad} differ from the reference pin's digests"
