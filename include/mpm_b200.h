@@ -87,6 +87,18 @@ const char* mpm_last_error(void);
 /* Number of visible CUDA devices (0 is not an error). */
 mpm_status mpm_device_count(int* count);
 
+/* Cap on the device memory this library holds at once, over every scene,
+ * batch and server of the process (no counterpart in the reference, where
+ * the browser's WebGPU device enforces its own limits).  0 (the default)
+ * means no cap.  An allocation that would pass it fails the way an
+ * exhausted device does: the call returns MPM_ERR_OOM and leaves its object
+ * as it was.  Lowering the cap frees nothing.  Use it to keep the library
+ * inside a share of the GPU, or to exercise out-of-memory paths. */
+mpm_status mpm_set_device_memory_limit(uint64_t bytes);
+
+/* Device bytes this library holds now (what the cap counts). */
+mpm_status mpm_device_memory_in_use(uint64_t* bytes);
+
 /* Grid sizing of the FluidGPU constructor (fluid-gpu.js:10-16):
  * grid_* = ceil(aspect_* / (4 * particle_radius)). */
 mpm_status mpm_desc_from_aspect(double aspect_x, double aspect_y, double aspect_z, double particle_radius,
@@ -141,8 +153,29 @@ mpm_status mpm_diffuse_set_gen_params(mpm_scene* scene, const mpm_gen_params* ge
 mpm_status mpm_step(mpm_scene* scene, int substeps);
 
 /* Wait for all work enqueued on the scene's stream, and for queued
- * alive-count readbacks. */
+ * alive-count readbacks.  Returns MPM_ERR_NAN when the scene's particle state
+ * holds a NaN or an infinity (MPM_HEALTH_NONFINITE below). */
 mpm_status mpm_sync(mpm_scene* scene);
+
+/* mpm_sync with a limit (no counterpart in the reference, whose frame loop
+ * never waits): waits at most timeout_s seconds (0: only looks) and returns
+ * MPM_ERR_TIMEOUT while the scene's work is still running, for a host loop
+ * that must not block, e.g. a renderer that skips a frame instead. */
+mpm_status mpm_wait(mpm_scene* scene, double timeout_s);
+
+/* Health of a scene (no counterpart in the reference, which reports
+ * nothing): bits kept on the device, set by the kernels and sticky until
+ * read with clear != 0.  Binned engine only (the plain engine reports 0).
+ *  MPM_HEALTH_NONFINITE: a particle's new position or velocity was NaN or
+ *    infinite (G2P).  A NaN position survives every clamp of the reference's
+ *    passes, so it never heals; mpm_sync and mpm_wait return MPM_ERR_NAN.
+ *  MPM_HEALTH_SATURATED: a P2G contribution reached encode's clamp of
+ *    +-20000 (shaders.js:17-24): the fixed-point grid no longer holds the
+ *    true sum, the usual sign of a simulation that has blown up.  Results
+ *    still follow the reference bit for bit; no call fails on it. */
+#define MPM_HEALTH_NONFINITE 1u
+#define MPM_HEALTH_SATURATED 2u
+mpm_status mpm_get_health(mpm_scene* scene, uint32_t* flags, int clear);
 
 /* Device pointer and byte size of a buffer in its reference layout (valid
  * until the next mpm_step; zero-copy hand-off to a consumer such as a
@@ -233,17 +266,23 @@ mpm_status mpm_compact(const mpm_ray_params* del, uint32_t n, const float* pos_i
 mpm_status mpm_raycast(const mpm_ray_params* ray, uint32_t n, const float* pos_in, uint32_t* hit_dev,
                        void* stream);
 
-/* Largest n mpm_compact_noalloc accepts (its scratch is a fixed 32 KB array). */
+/* Largest n mpm_compact_noalloc accepts (its scratch is a fixed array of
+ * 8,193 32-bit words, about 32 KB, one survivor count per 2,048 particles). */
 #define MPM_COMPACT_NOALLOC_MAX_N (1u << 24)
 
 /* No counterpart in the reference (whose COMPACT needs no scratch beyond its
  * atomic counter).  mpm_compact with the same arguments and results, but the
- * call allocates nothing: the per-block scratch is a fixed device array of
- * this library.  Runs on the current device.  n > MPM_COMPACT_NOALLOC_MAX_N
- * fails with MPM_ERR_CAPACITY before any work is enqueued.  The first call on
- * a device does a one-time setup (looks up the array's address), so make it
- * outside any stream capture.  Calls on one device share the scratch: calls
- * that can overlap in time (different streams, unordered threads) race. */
+ * call allocates nothing: for hosts that must not allocate device memory
+ * while they run (a real-time frame loop with a fixed memory plan, a caller
+ * whose allocator is someone else's, code running inside a stream capture),
+ * the per-block scratch is a fixed device array of this library instead of a
+ * stream-ordered allocation.  Runs on the current device.
+ * n > MPM_COMPACT_NOALLOC_MAX_N fails with MPM_ERR_CAPACITY before any work
+ * is enqueued; n = 0 only sets *count_dev to 0.  The first call on a device
+ * (and the first after its context was re-created, e.g. by cudaDeviceReset)
+ * looks up the array's address, so make it outside any stream capture.
+ * Calls on one device share the scratch: calls that can overlap in time
+ * (different streams, unordered threads) race. */
 mpm_status mpm_compact_noalloc(const mpm_ray_params* del, uint32_t n, const float* pos_in, const float* vel_in,
                                const float* mass_in, float* pos_out, float* vel_out, float* mass_out,
                                uint32_t* count_dev, void* stream);
@@ -347,7 +386,13 @@ mpm_status mpm_batch_set_hand(mpm_batch* batch, int32_t scene, const mpm_hand_pa
 
 /* Advances every scene by `substeps` substeps; enqueues and returns. */
 mpm_status mpm_batch_step(mpm_batch* batch, int substeps);
+
+/* Waits for the batch's stream; MPM_ERR_NAN when a live scene's state holds
+ * a NaN or an infinity (mpm_batch_get_health tells which). */
 mpm_status mpm_batch_sync(mpm_batch* batch);
+
+/* A scene's MPM_HEALTH_* bits, as mpm_get_health (waits for the stream). */
+mpm_status mpm_batch_get_health(mpm_batch* batch, int32_t scene, uint32_t* flags, int clear);
 
 /* Copies one buffer of one scene (reference layout, the scene's own particle
  * ids and grid) to host memory; waits. */
@@ -395,6 +440,7 @@ typedef struct mpm_job_result {
     double arrival_s, admit_s, finish_s;   /* server clock: seconds since mpm_server_run started */
     uint32_t n, substeps;
     int32_t done;
+    int32_t health;                        /* MPM_HEALTH_* bits of the job's scene at its last substep */
 } mpm_job_result;
 
 mpm_status mpm_server_create(const mpm_server_desc* desc, mpm_server** out);

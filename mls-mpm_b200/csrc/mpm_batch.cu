@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/mpm_b200.h"
+#include "mpm_alloc.h"
 #include "mpm_world.h"
 
 namespace mpm {
@@ -89,12 +90,15 @@ namespace mpm {
 // Staging for a scene of n particles (76 bytes each: an add uses 72, a
 // particle download 76), allocated before it is needed (the serving loop
 // reserves for its largest job before it starts).
+// Device address of a scene's health word (MPM_HEALTH_* bits).
+uint32_t* batch_health_word(mpm_batch* b, int32_t scene) { return b->w.health + scene; }
+
 cudaError_t batch_reserve_stage(mpm_batch* b, uint32_t n) {
     const size_t need = (size_t)(n ? n : 1) * 76;
     if (need <= b->stage_bytes) return cudaSuccess;
     const size_t bytes = std::max(need, (size_t)64 << 20);
     void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, bytes);
+    const cudaError_t e = dmalloc(&p, bytes);
     if (e != cudaSuccess) return e;
     if (b->stage) b->stage_old.push_back(b->stage);   // a queued import may still read it
     b->stage = p;
@@ -213,8 +217,8 @@ mpm_status mpm_batch_destroy(mpm_batch* b) {
     DevGuard g(b->device);
     cudaStream_t st = b->w.stream;
     world_free(b->w);   // waits for the stream
-    if (b->stage) cudaFree(b->stage);
-    for (void* p : b->stage_old) cudaFree(p);
+    dfree(b->stage);
+    for (void* p : b->stage_old) dfree(p);
     for (cudaEvent_t& e : b->tune.ev)
         if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
@@ -336,7 +340,22 @@ mpm_status mpm_batch_step(mpm_batch* b, int substeps) {
 mpm_status mpm_batch_sync(mpm_batch* b) {
     if (!b) return bfail(MPM_ERR_INVALID_ARG, "NULL argument");
     DevGuard g(b->device);
-    BATCH_TRY(cudaStreamSynchronize(b->w.stream), "mpm_batch_sync");
+    World& w = b->w;
+    BATCH_TRY(cudaStreamSynchronize(w.stream), "mpm_batch_sync");
+    // health of every live scene: one copy of the health words
+    std::vector<uint32_t> h(w.scene_cap ? w.scene_cap : 1, 0u);
+    BATCH_TRY(cudaMemcpy(h.data(), w.health, h.size() * 4, cudaMemcpyDeviceToHost), "health readback");
+    for (uint32_t i = 0; i < w.scene_cap; ++i)
+        if (w.scenes[i].live && (h[i] & MPM_HEALTH_NONFINITE))
+            return bfail(MPM_ERR_NAN, "scene " + std::to_string(i) +
+                                          " holds a NaN or an infinity (MPM_HEALTH_NONFINITE)");
+    return MPM_OK;
+}
+
+mpm_status mpm_batch_get_health(mpm_batch* b, int32_t scene, uint32_t* flags, int clear) {
+    if (!scene_ok(b, scene) || !flags) return bfail(MPM_ERR_INVALID_ARG, "unknown scene or NULL argument");
+    DevGuard g(b->device);
+    BATCH_TRY(world_read_health(b->w, scene, flags, clear != 0), "mpm_batch_get_health");
     return MPM_OK;
 }
 

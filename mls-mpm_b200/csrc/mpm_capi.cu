@@ -4,14 +4,17 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mpm_b200.h"
+#include "mpm_alloc.h"
 #include "mpm_edit.h"
 #include "mpm_kernels.h"
 #include "mpm_scene.h"
@@ -49,11 +52,7 @@ static mpm_status cuda_fail(cudaError_t e, const char* what) {
         if (_e != cudaSuccess) return cuda_fail(_e, what); \
     } while (0)
 
-template <class T> static cudaError_t dalloc(T** p, size_t bytes) {
-    *p = nullptr;
-    if (bytes == 0) bytes = 16;
-    return cudaMalloc((void**)p, bytes);
-}
+template <class T> static cudaError_t dalloc(T** p, size_t bytes) { return dmalloc(p, bytes); }
 
 cudaEvent_t Scene::take_event() {
     if (!event_pool.empty()) {
@@ -117,8 +116,7 @@ static void free_scene(Scene& s) {
                     s.diffuse.top_hist,
                     s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word, s.diffuse.gen_dev,
                     s.diffuse.adv_dev};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    for (void* p : ptrs) dfree(p);
     if (s.diffuse.host_top) cudaFreeHost(s.diffuse.host_top);
     if (s.diffuse.alive_ring) cudaFreeHost(s.diffuse.alive_ring);
     for (cudaEvent_t& ev : s.diffuse.alive_ev)
@@ -380,11 +378,29 @@ mpm_status mpm_destroy(mpm_scene* sc) {
     return MPM_OK;
 }
 
+// The plain engine indexes P2G_MOM's and G2P's stencils unchecked, as the
+// reference does (shaders.js:303-304, 598-599): every position must keep its
+// 3x3x3 stencil inside the grid, i.e. lie in [1, dim - 1) on each axis and be
+// finite.  The binned engine guards every stencil and takes any input.
+static mpm_status plain_positions_ok(const Scene& s, const float* pos4, uint32_t n) {
+    if (s.engine != kEnginePlain) return MPM_OK;
+    const float hi[3] = {(float)s.X - 1.0f, (float)s.Y - 1.0f, (float)s.Z - 1.0f};
+    for (uint32_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            const float x = pos4[4 * (size_t)i + a];
+            if (!(x >= 1.0f && x < hi[a]))
+                return fail(MPM_ERR_INVALID_ARG, "plain engine: particle " + std::to_string(i) +
+                                                     " lies outside [1, dim - 1) or is not finite");
+        }
+    return MPM_OK;
+}
+
 mpm_status mpm_upload_particles(mpm_scene* sc, const float* pos4, const float* vel4, const float* aff9,
                                 const float* mass, uint32_t n) {
     if (!sc || (!pos4 && n) || (!mass && n)) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     Scene& s = sc->s;
     if (n > s.capacity) return fail(MPM_ERR_CAPACITY, "n exceeds particle capacity");
+    if (const mpm_status bad = plain_positions_ok(s, pos4, n)) return bad;
     DeviceGuard guard(s.device);
     cudaStream_t st = s.stream;
     CUDA_TRY(cudaMemcpyAsync(s.pos, pos4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "upload pos");
@@ -517,12 +533,48 @@ mpm_status mpm_step(mpm_scene* sc, int substeps) {
     return MPM_OK;
 }
 
+// After the scene's stream has drained: MPM_ERR_NAN when its state went
+// non-finite (binned engine; the flag stays until mpm_get_health clears it).
+static mpm_status health_status(Scene& s) {
+    if (s.engine != kEngineBinned || s.world_slot < 0) return MPM_OK;
+    uint32_t flags = 0;
+    CUDA_TRY(world_read_health(s.world, s.world_slot, &flags, false), "health readback");
+    if (flags & MPM_HEALTH_NONFINITE)
+        return fail(MPM_ERR_NAN, "the scene's particle state holds a NaN or an infinity (MPM_HEALTH_NONFINITE)");
+    return MPM_OK;
+}
+
 mpm_status mpm_sync(mpm_scene* sc) {
     if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     DeviceGuard guard(sc->s.device);
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "mpm_sync");
     // queued alive-count readbacks have landed too
     if (sc->s.diffuse.rb_stream) CUDA_TRY(cudaStreamSynchronize(sc->s.diffuse.rb_stream), "mpm_sync readbacks");
+    return health_status(sc->s);
+}
+
+mpm_status mpm_wait(mpm_scene* sc, double timeout_s) {
+    if (!sc || !(timeout_s >= 0.0)) return fail(MPM_ERR_INVALID_ARG, "NULL scene or negative timeout");
+    DeviceGuard guard(sc->s.device);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(sc->s.stream);
+        if (e == cudaSuccess && sc->s.diffuse.rb_stream) e = cudaStreamQuery(sc->s.diffuse.rb_stream);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) return cuda_fail(e, "mpm_wait");
+        const double waited = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (waited >= timeout_s) return fail(MPM_ERR_TIMEOUT, "mpm_wait: the scene's work is still running");
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+    return health_status(sc->s);
+}
+
+mpm_status mpm_get_health(mpm_scene* sc, uint32_t* flags, int clear) {
+    if (!sc || !flags) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    *flags = 0;
+    if (sc->s.engine != kEngineBinned || sc->s.world_slot < 0) return MPM_OK;
+    DeviceGuard guard(sc->s.device);
+    CUDA_TRY(world_read_health(sc->s.world, sc->s.world_slot, flags, clear != 0), "mpm_get_health");
     return MPM_OK;
 }
 
@@ -593,6 +645,11 @@ mpm_status mpm_upload(mpm_scene* sc, mpm_buffer which, const void* host_src, siz
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_written = true;
     if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
+    if (which == MPM_BUF_POS && sc->s.engine == kEnginePlain) {
+        if (bytes % 16) return fail(MPM_ERR_INVALID_ARG, "plain engine: positions are uploaded as whole vec4 records");
+        if (const mpm_status bad = plain_positions_ok(sc->s, static_cast<const float*>(host_src), (uint32_t)(bytes / 16)))
+            return bad;
+    }
     DeviceGuard guard(sc->s.device);
     if (is_particle_buffer(which)) {
         CUDA_TRY(sync_reference_buffers(sc->s), "export");
@@ -696,7 +753,7 @@ static cudaError_t ensure_edit_scratch(Scene& s, bool compact) {
     if (e == cudaSuccess) e = dalloc(&s.edit_mass, N * 4);
     if (e == cudaSuccess) e = dalloc(&s.edit_blocks, compact_scratch_words(N) * 4);
     if (e != cudaSuccess) {
-        cudaFree(s.edit_pos); cudaFree(s.edit_vel); cudaFree(s.edit_mass); cudaFree(s.edit_blocks);
+        dfree(s.edit_pos); dfree(s.edit_vel); dfree(s.edit_mass); dfree(s.edit_blocks);
         s.edit_pos = nullptr; s.edit_vel = nullptr; s.edit_mass = nullptr; s.edit_blocks = nullptr;
     }
     return e;
@@ -763,6 +820,7 @@ mpm_status mpm_append_particles(mpm_scene* sc, const float* pos4, const float* v
     const uint32_t n = std::min<uint32_t>(count, s.capacity - start);   // fluid-gpu.js:147-149
     *appended = 0;
     if (n == 0) return MPM_OK;
+    if (const mpm_status bad = plain_positions_ok(s, pos4, n)) return bad;
     DeviceGuard guard(s.device);
     cudaStream_t st = s.stream;
     CUDA_TRY(sync_reference_buffers(s), "export");

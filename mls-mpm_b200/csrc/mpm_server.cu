@@ -30,6 +30,7 @@ void set_error(const std::string& msg);
 // Device staging of a batch (mpm_batch.cu) large enough to add a scene of n
 // particles without allocating then.
 cudaError_t batch_reserve_stage(mpm_batch* b, uint32_t n);
+uint32_t* batch_health_word(mpm_batch* b, int32_t scene);
 }
 
 namespace {
@@ -47,11 +48,16 @@ struct Job {
     int state = 0;                   // 0 queued, 1 active, 2 done
     std::vector<float> out_pos, out_vel, out_dens;
     const Clock::time_point* t0 = nullptr;
+    // the scene's health bits, copied at retirement into a pinned slot and
+    // from there into `health` by the stream-ordered host function
+    const volatile uint32_t* health_slot = nullptr;
+    volatile uint32_t health = 0;
 };
 
 void CUDART_CB stamp_finish(void* p) {
     Job* j = static_cast<Job*>(p);
     j->finish = std::chrono::duration<double>(Clock::now() - *j->t0).count();
+    if (j->health_slot) j->health = *j->health_slot;
 }
 
 mpm_status sfail(mpm_status st, const std::string& msg) {
@@ -113,6 +119,12 @@ struct mpm_server {
     uint32_t scap = 0;
     std::vector<std::unique_ptr<Job>> jobs;
     Clock::time_point t0;
+    // pinned ring of health words copied at job retirement; a slot is reused
+    // only after ring_size later retirements, by which time the host function
+    // that read it has run (the host stays at most max_inflight substeps
+    // ahead, each retiring at most scene_capacity jobs)
+    uint32_t* health_ring = nullptr;
+    uint32_t ring_size = 0, ring_next = 0;
 };
 
 extern "C" {
@@ -159,6 +171,14 @@ mpm_status mpm_server_create(const mpm_server_desc* d, mpm_server** out) {
         delete s;
         return st;
     }
+    s->ring_size = std::max<uint32_t>(4096u, S * (s->max_inflight + 2u));
+    if (cudaMallocHost((void**)&s->health_ring, (size_t)s->ring_size * 4) != cudaSuccess) {
+        cudaGetLastError();
+        mpm_batch_destroy(s->batch);
+        delete s;
+        return sfail(MPM_ERR_OOM, "pinned health ring");
+    }
+    std::memset(s->health_ring, 0, (size_t)s->ring_size * 4);
     *out = s;
     return MPM_OK;
 }
@@ -167,6 +187,7 @@ mpm_status mpm_server_destroy(mpm_server* s) {
     if (!s) return MPM_OK;
     mpm_batch_destroy(s->batch);   // waits for the batch's stream
     for (auto& j : s->jobs) release_inputs(*j);
+    if (s->health_ring) cudaFreeHost(s->health_ring);
     delete s;
     return MPM_OK;
 }
@@ -285,6 +306,11 @@ mpm_status mpm_server_run(mpm_server* s, mpm_server_stats* stats) {
                 active[w++] = j;
                 continue;
             }
+            uint32_t* slot_h = s->health_ring + (s->ring_next++ % s->ring_size);
+            if (cudaMemcpyAsync(slot_h, mpm::batch_health_word(s->batch, j->sid), 4, cudaMemcpyDeviceToHost,
+                                stream) != cudaSuccess)
+                return sfail(MPM_ERR_DEVICE, "health copy");
+            j->health_slot = slot_h;
             if (cudaLaunchHostFunc(stream, stamp_finish, j) != cudaSuccess) return sfail(MPM_ERR_DEVICE, "host func");
             if (keep) {
                 j->out_pos.resize((size_t)j->n * 4);
@@ -349,6 +375,7 @@ mpm_status mpm_server_job(mpm_server* s, int64_t job, mpm_job_result* out) {
     out->n = j.n;
     out->substeps = j.substeps;
     out->done = j.state == 2;
+    out->health = j.state == 2 ? (int32_t)j.health : 0;
     return MPM_OK;
 }
 

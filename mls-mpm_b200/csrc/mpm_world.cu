@@ -45,6 +45,7 @@
 #include <cstdint>
 #include <cstring>
 
+#include "mpm_alloc.h"
 #include "mpm_device.cuh"
 #include "mpm_kernels.h"
 #include "mpm_scene.h"
@@ -109,6 +110,7 @@ WorldView World::view() const {
     v.chunk_info = chunk_info; v.chunk_last = chunk_last; v.chunk_hdr = chunk_hdr; v.chunk_geo = chunk_geo;
     v.tile_occ_list = tile_occ_list; v.tile_grid_list = tile_grid_list;
     v.ctrl = ctrl; v.dens = dens;
+    v.health = health;
     return v;
 }
 
@@ -668,27 +670,29 @@ __device__ __forceinline__ bool halo_cell(const ChunkHdr& h, const SceneDesc& sd
 // slot hb, written out through template indices (immediate offsets, no
 // per-cell control flow).  kClamp: encode with its clamp.
 template <bool kClamp, int K, int J, int I>
-__device__ __forceinline__ void mass_cell(const PW& w, float m, int32_t* a) {
+__device__ __forceinline__ void mass_cell(const PW& w, float m, int32_t* a, uint32_t& sat) {
     const float x = w.wx[I] * w.wy[J] * w.wz[K] * m;
-    atomicAdd(a + (K * kHXY + J * kHX + I), kClamp ? encode(x) : encode_unclamped(x));
+    const int32_t e = kClamp ? encode(x) : encode_unclamped(x);
+    if (kClamp) sat |= at_clamp(e);
+    atomicAdd(a + (K * kHXY + J * kHX + I), e);
 }
 template <bool kClamp, int K, int J>
-__device__ __forceinline__ void mass_row(const PW& w, float m, int32_t* a) {
-    mass_cell<kClamp, K, J, 0>(w, m, a);
-    mass_cell<kClamp, K, J, 1>(w, m, a);
-    mass_cell<kClamp, K, J, 2>(w, m, a);
+__device__ __forceinline__ void mass_row(const PW& w, float m, int32_t* a, uint32_t& sat) {
+    mass_cell<kClamp, K, J, 0>(w, m, a, sat);
+    mass_cell<kClamp, K, J, 1>(w, m, a, sat);
+    mass_cell<kClamp, K, J, 2>(w, m, a, sat);
 }
 template <bool kClamp>
-__device__ __forceinline__ void mass_contrib_shared(const PW& w, float m, int32_t* a) {
-    mass_row<kClamp, 0, 0>(w, m, a);
-    mass_row<kClamp, 0, 1>(w, m, a);
-    mass_row<kClamp, 0, 2>(w, m, a);
-    mass_row<kClamp, 1, 0>(w, m, a);
-    mass_row<kClamp, 1, 1>(w, m, a);
-    mass_row<kClamp, 1, 2>(w, m, a);
-    mass_row<kClamp, 2, 0>(w, m, a);
-    mass_row<kClamp, 2, 1>(w, m, a);
-    mass_row<kClamp, 2, 2>(w, m, a);
+__device__ __forceinline__ void mass_contrib_shared(const PW& w, float m, int32_t* a, uint32_t& sat) {
+    mass_row<kClamp, 0, 0>(w, m, a, sat);
+    mass_row<kClamp, 0, 1>(w, m, a, sat);
+    mass_row<kClamp, 0, 2>(w, m, a, sat);
+    mass_row<kClamp, 1, 0>(w, m, a, sat);
+    mass_row<kClamp, 1, 1>(w, m, a, sat);
+    mass_row<kClamp, 1, 2>(w, m, a, sat);
+    mass_row<kClamp, 2, 0>(w, m, a, sat);
+    mass_row<kClamp, 2, 1>(w, m, a, sat);
+    mass_row<kClamp, 2, 2>(w, m, a, sat);
 }
 
 // ---------------------------------------------------------------------------
@@ -711,6 +715,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     // the accumulators start at zero and every flush zeroes what it read
     for (int i = threadIdx.x; i < kHaloCells; i += blockDim.x) acc[i] = 0;
     __syncthreads();
+    uint32_t sat = 0;   // a contribution of this thread's particles hit encode's clamp in this chunk
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         const ChunkHdr h = hs;
         const uint32_t nxt = ch + gridDim.x;
@@ -741,8 +746,8 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             if (fast) {
                 // weight <= 0.4219: for |mass| < 47000 encode's clamp is the identity
                 const bool safe = fabsf(q[r].w) < 47000.0f;
-                if (safe) mass_contrib_shared<false>(w, q[r].w, acc + hb);
-                else mass_contrib_shared<true>(w, q[r].w, acc + hb);
+                if (safe) mass_contrib_shared<false>(w, q[r].w, acc + hb, sat);
+                else mass_contrib_shared<true>(w, q[r].w, acc + hb, sat);
             } else if (valid) {
                 // stencil outside the halo or the grid: bounds-checked global atomics
                 const int32_t X = sd.X, Y = sd.Y, Z = sd.Z;
@@ -753,11 +758,14 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
                             const int32_t xx = w.cx - 1 + i, yy = w.cy - 1 + j, zz = w.cz - 1 + kk;
                             if (xx < 0 || xx >= X || yy < 0 || yy >= Y || zz < 0 || zz >= Z) continue;
                             const float ww = w.wx[i] * w.wy[j] * w.wz[kk];
-                            atomicAdd(&scm[(zz * Y + yy) * X + xx], encode(ww * q[r].w));
+                            const int32_t e = encode(ww * q[r].w);
+                            sat |= at_clamp(e);
+                            atomicAdd(&scm[(zz * Y + yy) * X + xx], e);
                         }
             }
         }
-        __syncthreads();
+        if (__syncthreads_or((int)sat) && threadIdx.x == 0) atomicOr(&v.health[h.scene], MPM_HEALTH_SATURATED);
+        sat = 0;
         // every thread holds this chunk's header: the next one can replace it
         if (threadIdx.x == 0 && nxt < nch) chunk_header_from(nci, nlast, ngeo, hs);
         int32_t* scm = cm + sd.cell_base;
@@ -965,7 +973,7 @@ struct MomTerms {
 template <bool kClamp, int K, int J, int I>
 __device__ __forceinline__ void mom_cell(const PW& w, const MomIn& in, const MomTerms& t, float qx, float qy,
                                          float qzz, float gx, float gy, float gz, int32_t* a0, int32_t* a1,
-                                         int32_t* a2) {
+                                         int32_t* a2, uint32_t& sat) {
     const float ww = w.wx[I] * (w.wy[J] * w.wz[K]);
     const float Qx = qx + t.qz[0][K];
     const float Qy = qy + t.qz[1][K];
@@ -977,14 +985,18 @@ __device__ __forceinline__ void mom_cell(const PW& w, const MomIn& in, const Mom
     const float vy = ww * (in.m * (in.vy + Qy) + fyf);
     const float vz = ww * (in.m * (in.vz + Qz) + fzf);
     constexpr int o = K * kHXY + J * kHX + I;
-    atomicAdd(a0 + o, kClamp ? encode(vx) : encode_unclamped(vx));
-    atomicAdd(a1 + o, kClamp ? encode(vy) : encode_unclamped(vy));
-    atomicAdd(a2 + o, kClamp ? encode(vz) : encode_unclamped(vz));
+    const int32_t ex = kClamp ? encode(vx) : encode_unclamped(vx);
+    const int32_t ey = kClamp ? encode(vy) : encode_unclamped(vy);
+    const int32_t ez = kClamp ? encode(vz) : encode_unclamped(vz);
+    if (kClamp) sat |= at_clamp(ex) | at_clamp(ey) | at_clamp(ez);
+    atomicAdd(a0 + o, ex);
+    atomicAdd(a1 + o, ey);
+    atomicAdd(a2 + o, ez);
 }
 
 template <bool kClamp, int J, int I>
 __device__ __forceinline__ void mom_column(const PW& w, const MomIn& in, const MomTerms& t, int32_t* a0,
-                                           int32_t* a1, int32_t* a2) {
+                                           int32_t* a1, int32_t* a2, uint32_t& sat) {
     const float dxi = t.dxs[I], dyj = t.dys[J];
     const float qx = in.a00 * dxi + in.a01 * dyj;
     const float qy = in.a10 * dxi + in.a11 * dyj;
@@ -992,14 +1004,14 @@ __device__ __forceinline__ void mom_column(const PW& w, const MomIn& in, const M
     const float gx = t.s00 * dxi + t.s01 * dyj;
     const float gy = t.s01 * dxi + t.s11 * dyj;
     const float gz = t.s02 * dxi + t.s12 * dyj;
-    mom_cell<kClamp, 0, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
-    mom_cell<kClamp, 1, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
-    mom_cell<kClamp, 2, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
+    mom_cell<kClamp, 0, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2, sat);
+    mom_cell<kClamp, 1, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2, sat);
+    mom_cell<kClamp, 2, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2, sat);
 }
 
 template <bool kClamp>
 __device__ __forceinline__ void mom_contrib_shared(const PW& w, const MomIn& in, const float* s, float coef,
-                                                   int32_t (*acc)[kHaloCells], int hb) {
+                                                   int32_t (*acc)[kHaloCells], int hb, uint32_t& sat) {
     MomTerms t;
     t.s00 = s[0]; t.s11 = s[1]; t.s01 = s[3]; t.s02 = s[4]; t.s12 = s[5];
     const float s22 = s[2];
@@ -1019,15 +1031,15 @@ __device__ __forceinline__ void mom_contrib_shared(const PW& w, const MomIn& in,
     int32_t* a0 = &acc[0][hb];
     int32_t* a1 = &acc[1][hb];
     int32_t* a2 = &acc[2][hb];
-    mom_column<kClamp, 0, 0>(w, in, t, a0, a1, a2);
-    mom_column<kClamp, 0, 1>(w, in, t, a0, a1, a2);
-    mom_column<kClamp, 0, 2>(w, in, t, a0, a1, a2);
-    mom_column<kClamp, 1, 0>(w, in, t, a0, a1, a2);
-    mom_column<kClamp, 1, 1>(w, in, t, a0, a1, a2);
-    mom_column<kClamp, 1, 2>(w, in, t, a0, a1, a2);
-    mom_column<kClamp, 2, 0>(w, in, t, a0, a1, a2);
-    mom_column<kClamp, 2, 1>(w, in, t, a0, a1, a2);
-    mom_column<kClamp, 2, 2>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 0, 0>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 0, 1>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 0, 2>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 1, 0>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 1, 1>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 1, 2>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 2, 0>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 2, 1>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 2, 2>(w, in, t, a0, a1, a2, sat);
 }
 
 // Density of one particle from the staged halo masses (shaders.js:305-313):
@@ -1062,7 +1074,7 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
                                              uint32_t p, const float4 pm, const float4 vi, const float* a,
                                              const float* mh, int32_t (*acc)[kHaloCells],
                                              const float* __restrict__ scmf, int32_t* __restrict__ smv,
-                                             float* __restrict__ dens) {
+                                             float* __restrict__ dens, uint32_t& sat) {
     const uint32_t X = sd.X, SLICE = sd.X * sd.Y, G = sd.G;
     const PW w = particle_weights(pm.x, pm.y, pm.z);
     const bool fast = valid && in_halo(w, h, sd);
@@ -1110,10 +1122,11 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
                      ac * 1.5f * (fabsf(s[4]) + fabsf(s[5]) + fabsf(s[2]));
     const bool safe = fmaxf(bx, fmaxf(by, bz)) * 0.4222f < 19000.0f;
     if (live && fast) {
-        if (safe) mom_contrib_shared<false>(w, in, s, coef, acc, hb);
-        else mom_contrib_shared<true>(w, in, s, coef, acc, hb);
+        if (safe) mom_contrib_shared<false>(w, in, s, coef, acc, hb, sat);
+        else mom_contrib_shared<true>(w, in, s, coef, acc, hb, sat);
     } else if (live) {
         auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
+            sat |= at_clamp(ex) | at_clamp(ey) | at_clamp(ez);
             const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
             if (cidx < G) {
                 atomicAdd(smv + 3ull * cidx + 0, ex);
@@ -1200,6 +1213,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
     cp_async_wait();
     __syncthreads();
     int b = 0;
+    uint32_t sat = 0;   // a contribution of this thread's particles hit encode's clamp in this chunk
     for (uint32_t ch = blockIdx.x; ch < nch; ch += G) {
         const ChunkHdr h = hdr[b];
         const uint32_t nxt = ch + G, nxt2 = nxt + G;
@@ -1231,7 +1245,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
             float4 pmn = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vin = pmn;
             float an[9];
             mom_load(v, pn, vn, posm, velid, aff, plane, pmn, vin, an);
-            mom_particle(v, h, sd, valid, p, pm, vi, a, mh[b], acc, scmf, smv, dens);
+            mom_particle(v, h, sd, valid, p, pm, vi, a, mh[b], acc, scmf, smv, dens, sat);
             p = pn;
             valid = vn;
             pm = pmn;
@@ -1239,7 +1253,8 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
 #pragma unroll
             for (int e = 0; e < 9; ++e) a[e] = an[e];
         }
-        __syncthreads();
+        if (__syncthreads_or((int)sat) && threadIdx.x == 0) atomicOr(&v.health[h.scene], MPM_HEALTH_SATURATED);
+        sat = 0;
         // hdr[b] is free: the header two chunks ahead goes there
         if (threadIdx.x == 0 && nxt2 < nch) hdr[b] = unpack_header(nh0, nh1);
         const int hn = halo_span(h);
@@ -1483,11 +1498,16 @@ struct G2POut {
 // so the atomic's round trip overlaps later work).
 __device__ __forceinline__ uint32_t g2p_store(const G2POut& o, const SceneDesc& sd, uint32_t p, const float4 q,
                                               const float4 vi, float density, float gvx, float gvy, float gvz,
-                                              const float* B) {
+                                              const float* B, uint32_t& bad) {
 #pragma unroll
     for (int e = 0; e < 9; ++e) o.aff[e * o.plane + p] = B[e] * 4.0f;
     f3 np, nv;
     g2p_finish(q, gvx, gvy, gvz, sd.P, sd.W, np, nv);
+    // health: a NaN or an infinity in the new state shows in the sum (positions
+    // are clamped to the grid and velocities stay below ~1e10, so a finite
+    // state cannot overflow it)
+    const float hs = ((np.x + np.y) + (np.z + nv.x)) + (nv.y + nv.z);
+    bad |= !(fabsf(hs) <= 3.0e38f) ? 1u : 0u;
     o.posm[p] = make_float4(np.x, np.y, np.z, q.w);
     o.velid[p] = make_float4(nv.x, nv.y, nv.z, vi.w);
     // binning of the new position
@@ -1519,12 +1539,15 @@ __device__ __forceinline__ uint32_t g2p_store(const G2POut& o, const SceneDesc& 
 
 // G2P of a particle whose stencil leaves the halo box or the grid (rare): the
 // reference's linear stencil index with a bounds guard, then the epilogue.
-__device__ __noinline__ void g2p_direct_particle(const G2POut o, const SceneDesc* sdp, uint32_t p, const float4 q,
-                                                 const float4 vi, const float4* __restrict__ vel4) {
+// Returns 1 when the new state is not finite.
+__device__ __noinline__ uint32_t g2p_direct_particle(const G2POut o, const SceneDesc* sdp, uint32_t p, const float4 q,
+                                                     const float4 vi, const float4* __restrict__ vel4) {
     const SceneDesc& sd = *sdp;
     const PW w = particle_weights(q.x, q.y, q.z);
     const G2PSum r = g2p_gather_direct(w, q, vel4, sd.X, sd.Y, sd.G);
-    o.rank[p] = g2p_store(o, sd, p, q, vi, o.dens[p], r.gv[0], r.gv[1], r.gv[2], r.B);
+    uint32_t bad = 0;
+    o.rank[p] = g2p_store(o, sd, p, q, vi, o.dens[p], r.gv[0], r.gv[1], r.gv[2], r.B, bad);
+    return bad;
 }
 
 template <uint32_t kC>
@@ -1545,6 +1568,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     uint32_t cached = kHole;
     // rank of the last particle whose atomic is still in flight
     uint32_t pend_p = kHole, pend_rank = 0;
+    uint32_t bad = 0;   // this thread saw a non-finite new state in the current chunk
     const float bubble_min = dv.enabled ? dv.gen->density_bubble_min : 0.0f;
     const float pressure_threshold = dv.enabled ? dv.gen->pressure_threshold : 0.0f;
     const float ke_threshold = dv.enabled ? dv.gen->ke_threshold : 0.0f;
@@ -1609,7 +1633,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
             const float4 vi = make_float4(0.0f, 0.0f, 0.0f, ids[r]);
             const PW w = particle_weights(q.x, q.y, q.z);
             if (!in_halo(w, h, sd)) {
-                g2p_direct_particle(out, &sd, p, q, vi, svel);
+                bad |= g2p_direct_particle(out, &sd, p, q, vi, svel);
                 continue;
             }
             float gvx = 0.0f, gvy = 0.0f, gvz = 0.0f;
@@ -1639,13 +1663,15 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
                     }
                 }
             }
-            const uint32_t rk = g2p_store(out, sd, p, q, vi, dns[r], gvx, gvy, gvz, B);
+            const uint32_t rk = g2p_store(out, sd, p, q, vi, dns[r], gvx, gvy, gvz, B, bad);
             // the previous particle's rank: its atomic has long returned
             if (pend_p != kHole) v.rank[pend_p] = pend_rank;
             pend_p = p;
             pend_rank = rk;
         }
-        __syncthreads();
+        // the chunk's scene is flagged once if any of its particles went non-finite
+        if (__syncthreads_or((int)bad) && threadIdx.x == 0) atomicOr(&v.health[h.scene], MPM_HEALTH_NONFINITE);
+        bad = 0;
     }
     if (pend_p != kHole) v.rank[pend_p] = pend_rank;
 }
@@ -1707,6 +1733,7 @@ template <class F> static void world_arrays(World& w, F&& f) {
     f(w.mvf, C * 12);
     f(w.vel4, C * 16);
     f(w.d_scenes, (size_t)w.scene_cap * sizeof(SceneDesc));
+    f(w.health, (size_t)(w.scene_cap ? w.scene_cap : 1) * 4);
 }
 
 uint64_t world_footprint(uint32_t particle_cap, uint64_t cell_cap, uint32_t scene_cap) {
@@ -1740,7 +1767,7 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
     cudaError_t e = cudaSuccess;
     w.device_bytes = 0;
     world_arrays(w, [&](auto*& p, size_t bytes) {
-        if (e == cudaSuccess) e = cudaMalloc((void**)&p, bytes ? bytes : 16);
+        if (e == cudaSuccess) e = dmalloc(&p, bytes);
         if (e == cudaSuccess) w.device_bytes += bytes;
     });
     if (e != cudaSuccess) return e;
@@ -1761,6 +1788,7 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
     if (e == cudaSuccess) e = cudaMemsetAsync(w.tile_occ, 0, T * 4, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.dens, 0, P * 4, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.ctrl, 0, sizeof(Ctrl), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.health, 0, (size_t)(scene_cap ? scene_cap : 1) * 4, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.key, 0xFF, P * 4, stream);
     // every permutation entry always names a valid position, even if a bug left one unwritten
     if (e == cudaSuccess) e = cudaMemsetAsync(w.perm, 0, P * 4, stream);
@@ -1782,7 +1810,7 @@ void world_free(World& w) {
     for (int b = 0; b < 2; ++b)
         if (w.graph[b]) cudaGraphExecDestroy(w.graph[b]);
     world_arrays(w, [](auto*& p, size_t) {
-        if (p) cudaFree((void*)p);
+        dfree(p);
         p = nullptr;
     });
     w = World();
@@ -1895,6 +1923,7 @@ cudaError_t world_add_scene(World& w, uint32_t X, uint32_t Y, uint32_t Z, const 
     for (uint32_t t = 0; t < nt; ++t) w.h_tile_scene[tb + t] = (uint32_t)slot;
     e = cudaMemcpyAsync(w.tile_scene + tb, w.h_tile_scene.data() + tb, (size_t)nt * 4, cudaMemcpyHostToDevice,
                         w.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.health + slot, 0, 4, w.stream);   // a new scene starts healthy
     if (e == cudaSuccess) e = world_upload_table(w);
     if (e != cudaSuccess) return e;
     if (n) {
@@ -1925,6 +1954,15 @@ void world_scene_grid(const World& w, int slot, int32_t** cm, int32_t** mv, floa
     if (mv) *mv = w.cm_current + w.cell_cap + 3ull * r.cell_base;
     if (cmf) *cmf = w.cmf + r.cell_base;
     if (mvf) *mvf = w.mvf + 3ull * r.cell_base;
+}
+
+cudaError_t world_read_health(World& w, int slot, uint32_t* flags, bool clear) {
+    *flags = 0;
+    if (slot < 0 || slot >= (int)w.scene_cap) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemcpyAsync(flags, w.health + slot, 4, cudaMemcpyDeviceToHost, w.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w.stream);
+    if (e == cudaSuccess && clear && *flags) e = cudaMemsetAsync(w.health + slot, 0, 4, w.stream);
+    return e;
 }
 
 cudaError_t world_remove_scene(World& w, int slot) {

@@ -101,6 +101,7 @@ struct WorldView {
     uint32_t* tile_grid_list;
     Ctrl* ctrl;
     float* dens;               // npos, layout of the last substep
+    uint32_t* health;          // per scene slot: MPM_HEALTH_* bits (sticky until read with clear)
 };
 
 // Diffuse spawn staging for the one scene of a world that has diffuse on.
@@ -199,6 +200,7 @@ struct World {
     float* cmf = nullptr;                        // cells
     float* mvf = nullptr;                        // 3 cells
     float4* vel4 = nullptr;                      // cells: (vx, vy, vz, 0), the same velocities 16-byte aligned
+    uint32_t* health = nullptr;                  // scene_cap words: MPM_HEALTH_* bits per scene slot
 
     // CUDA graphs of one substep (one per buffer parity), valid for `generation`
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -226,6 +228,9 @@ cudaError_t world_remove_scene(World& w, int slot);
 cudaError_t world_export_scene(World& w, int slot, float4* pos, float4* vel, float* aff, float* mass, float* dens);
 // Grid buffers of a scene (reference layouts) inside the world arrays.
 void world_scene_grid(const World& w, int slot, int32_t** cm, int32_t** mv, float** cmf, float** mvf);
+// A scene's MPM_HEALTH_* bits as of the work enqueued so far (waits for the
+// world's stream); clear: reset them afterwards (in stream order).
+cudaError_t world_read_health(World& w, int slot, uint32_t* flags, bool clear);
 cudaError_t world_upload_table(World& w);
 // Sets a scene's uniforms (Params, WallParams, HandParams + dispatch dims;
 // hand_dims null or active == 0: no APPLY_HAND).  Takes effect at the next substep.

@@ -208,7 +208,16 @@ SIGNATURES = {
     "mpm_server_run": (_I, [_V, _V]),
     "mpm_server_job": (_I, [_V, ctypes.c_int64, _V]),
     "mpm_server_download": (_I, [_V, ctypes.c_int64, _I, _V, _SZ]),
+    "mpm_wait": (_I, [_V, ctypes.c_double]),
+    "mpm_set_device_memory_limit": (_I, [_U64]),
+    "mpm_device_memory_in_use": (_I, [ctypes.POINTER(_U64)]),
+    "mpm_get_health": (_I, [_V, ctypes.POINTER(_U32), _I]),
+    "mpm_batch_get_health": (_I, [_V, ctypes.c_int32, ctypes.POINTER(_U32), _I]),
 }
+
+# MPM_HEALTH_* bits (mpm_get_health, mpm_batch_get_health, JobResult.health)
+HEALTH_NONFINITE = 1
+HEALTH_SATURATED = 2
 
 SERVER_KEEP_STATE = 0x100
 
@@ -230,7 +239,8 @@ class ServerStats(ctypes.Structure):
 
 class JobResult(ctypes.Structure):
     _fields_ = [("arrival_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("finish_s", ctypes.c_double),
-                ("n", ctypes.c_uint32), ("substeps", ctypes.c_uint32), ("done", ctypes.c_int32)]
+                ("n", ctypes.c_uint32), ("substeps", ctypes.c_uint32), ("done", ctypes.c_int32),
+                ("health", ctypes.c_int32)]
 
 BATCH_NO_GRAPH = 1
 BATCH_AUTOTUNE = 2

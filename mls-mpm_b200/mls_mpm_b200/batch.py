@@ -64,6 +64,13 @@ class Batch:
     def sync(self):
         check(self.lib.mpm_batch_sync(self.h), "mpm_batch_sync")
 
+    def health(self, sid, clear=False):
+        """MPM_HEALTH_* bits of one scene (mpm_batch_get_health)."""
+        f = ctypes.c_uint32()
+        check(self.lib.mpm_batch_get_health(self.h, int(sid), ctypes.byref(f), int(bool(clear))),
+              "mpm_batch_get_health")
+        return f.value
+
     def stream(self):
         s = ctypes.c_void_p()
         check(self.lib.mpm_batch_get_stream(self.h, ctypes.byref(s)), "mpm_batch_get_stream")

@@ -12,7 +12,7 @@ from .abi import LIB_PATH, PKG_DIR
 CSRC = os.path.join(os.path.dirname(PKG_DIR), "csrc")
 INCLUDE = os.path.join(os.path.dirname(os.path.dirname(PKG_DIR)), "include")
 
-SOURCES = ["mpm_capi.cu", "mpm_kernels.cu", "mpm_world.cu", "mpm_edit.cu", "mpm_noalloc.cu", "mpm_batch.cu", "mpm_server.cu"]
+SOURCES = ["mpm_alloc.cu", "mpm_capi.cu", "mpm_kernels.cu", "mpm_world.cu", "mpm_edit.cu", "mpm_noalloc.cu", "mpm_batch.cu", "mpm_server.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "--expt-relaxed-constexpr"]

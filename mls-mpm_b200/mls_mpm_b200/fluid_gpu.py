@@ -232,6 +232,21 @@ class FluidGPU:
     def sync(self):
         check(self._lib.mpm_sync(self._scene), "mpm_sync")
 
+    def wait(self, timeout_s):
+        """True once the scene's work is done, False while it still runs after
+        timeout_s seconds (mpm_wait); raises on a non-finite state."""
+        st = self._lib.mpm_wait(self._scene, float(timeout_s))
+        if st == 4:   # MPM_ERR_TIMEOUT
+            return False
+        check(st, "mpm_wait")
+        return True
+
+    def health(self, clear=False):
+        """MPM_HEALTH_* bits of the scene (abi.HEALTH_NONFINITE, abi.HEALTH_SATURATED)."""
+        f = ctypes.c_uint32()
+        check(self._lib.mpm_get_health(self._scene, ctypes.byref(f), int(bool(clear))), "mpm_get_health")
+        return f.value
+
     # ---- buffers ----
     def get_buffer(self, name):
         """(device pointer, bytes) of a reference-layout buffer."""
