@@ -166,20 +166,32 @@ mpm_status mpm_wait(mpm_scene* scene, double timeout_s);
 /* Health of a scene (no counterpart in the reference, which reports
  * nothing): bits kept on the device, set by the kernels and sticky until
  * read with clear != 0.  Binned engine only (the plain engine reports 0).
- *  MPM_HEALTH_NONFINITE: a particle's new position or velocity was NaN or
- *    infinite (G2P).  A NaN position survives every clamp of the reference's
- *    passes, so it never heals; mpm_sync and mpm_wait return MPM_ERR_NAN.
- *  MPM_HEALTH_SATURATED: a P2G contribution reached encode's clamp of
- *    +-20000 (shaders.js:17-24): the fixed-point grid no longer holds the
- *    true sum, the usual sign of a simulation that has blown up.  Results
- *    still follow the reference bit for bit; no call fails on it. */
+ *  MPM_HEALTH_NONFINITE: a particle position was NaN or infinite at the
+ *    start of a substep (P2G_MASS).  A NaN position survives every clamp of
+ *    the reference's passes, so it never heals (velocities cannot stay
+ *    non-finite: the next P2G clamps them); mpm_sync and mpm_wait return
+ *    MPM_ERR_NAN.
+ *  MPM_HEALTH_SATURATED: encode's clamp of +-20000 (shaders.js:17-24) could
+ *    engage, so the fixed-point grid may no longer hold the true sum, the
+ *    usual sign of a simulation that has blown up.  Set for a particle whose
+ *    bound on its P2G contributions passes about 45,000: every real clamp is
+ *    flagged, and near misses too.  Results still follow the reference bit
+ *    for bit; no call fails on it. */
 #define MPM_HEALTH_NONFINITE 1u
 #define MPM_HEALTH_SATURATED 2u
 mpm_status mpm_get_health(mpm_scene* scene, uint32_t* flags, int clear);
 
-/* Device pointer and byte size of a buffer in its reference layout (valid
- * until the next mpm_step; zero-copy hand-off to a consumer such as a
- * renderer's vertex input, fluid-renderer.js:315-328). */
+/* Device pointer and byte size of a buffer in its reference layout, for a
+ * zero-copy consumer such as a renderer's vertex inputs
+ * (fluid-renderer.js:315-328).  The pointer stays valid for the scene's life.
+ * Contents, in stream order (read after mpm_sync, or order work after the
+ * scene's stream):
+ *  - MPM_BUF_POS, MPM_BUF_VEL, MPM_BUF_DENSITY: the first such call makes
+ *    every later substep write these three in place (a renderer reads them
+ *    every frame), so they follow each step with no further call;
+ *  - MPM_BUF_AFFINE, MPM_BUF_MASS: as of this call, until the next mpm_step;
+ *  - grid and diffuse buffers: always current.  The diffuse pool is for
+ *    reading: write it with mpm_upload (ADVECT keeps an index of live slots). */
 mpm_status mpm_get_buffer(mpm_scene* scene, mpm_buffer which, void** dev_ptr, size_t* bytes);
 
 /* Zero-copy export of a buffer (reference layout) to another process on the

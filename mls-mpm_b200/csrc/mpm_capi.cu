@@ -111,7 +111,8 @@ static void free_scene(Scene& s) {
     }
     void* ptrs[] = {s.pos, s.vel, s.aff, s.mass, s.dens, s.grid_i32, s.cmf, s.mvf,
                     s.diffuse.pool, s.diffuse.free_list, s.diffuse.top, s.diffuse.spawn_bits,
-                    s.diffuse.kill_bits, s.diffuse.block_counts, s.diffuse.kill_counts, s.diffuse.rank_state,
+                    s.diffuse.kill_bits, s.diffuse.alive_mask, s.diffuse.block_counts, s.diffuse.kill_counts,
+                    s.diffuse.rank_state,
                     s.diffuse.staging,
                     s.diffuse.top_hist,
                     s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word, s.diffuse.gen_dev,
@@ -180,6 +181,17 @@ static cudaError_t sync_reference_buffers(Scene& s) {
     cudaError_t e = world_export_scene(s.world, s.world_slot, s.pos, s.vel, s.aff, s.mass, s.dens);
     if (e == cudaSuccess) s.ref_stale = false;
     return e;
+}
+
+// The buffers a renderer reads every frame (fluid-renderer.js:315-328).
+static bool render_buffer(mpm_buffer w) { return w == MPM_BUF_POS || w == MPM_BUF_VEL || w == MPM_BUF_DENSITY; }
+
+// Binned engine: make one reference-layout particle buffer current.  Once the
+// substeps mirror pos/vel/density (Scene::mirror), those three need nothing.
+static cudaError_t ensure_reference(Scene& s, mpm_buffer which) {
+    if (s.engine != kEngineBinned || !is_particle_buffer(which)) return cudaSuccess;
+    if (s.mirror && render_buffer(which)) return cudaSuccess;
+    return sync_reference_buffers(s);
 }
 
 // Binned engine: (re)load the working state from the reference-layout buffers.
@@ -467,6 +479,7 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     if (e == cudaSuccess) e = dalloc(&d.top, 16);
     if (e == cudaSuccess) e = dalloc(&d.spawn_bits, nwN * 4);
     if (e == cudaSuccess) e = dalloc(&d.kill_bits, nwM * 4);
+    if (e == cudaSuccess) e = dalloc(&d.alive_mask, nwM * 4);
     if (e == cudaSuccess) e = dalloc(&d.block_counts, nb * 4);
     if (e == cudaSuccess) e = dalloc(&d.kill_counts, nb * 4);
     if (e == cudaSuccess) e = dalloc(&d.rank_state, 32);
@@ -488,6 +501,7 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     CUDA_TRY(cudaMemcpyAsync(d.free_list, fl.data(), M * 4, cudaMemcpyHostToDevice, s.stream), "free list");
     CUDA_TRY(cudaMemcpyAsync(d.top, &top, 4, cudaMemcpyHostToDevice, s.stream), "top");
     CUDA_TRY(cudaMemsetAsync(d.pool, 0, M * 48, s.stream), "pool");
+    CUDA_TRY(cudaMemsetAsync(d.alive_mask, 0, nwM * 4, s.stream), "alive mask");
     CUDA_TRY(cudaMemsetAsync(d.rank_state, 0, 32, s.stream), "free-list pass state");
     // the spawn bits and counts start clear; each kill pass clears them again
     CUDA_TRY(cudaMemsetAsync(d.spawn_bits, 0, nwN * 4, s.stream), "spawn bits");
@@ -583,8 +597,15 @@ mpm_status mpm_get_buffer(mpm_scene* sc, mpm_buffer which, void** dev_ptr, size_
     if (!buffer_info(sc->s, which, dev_ptr, bytes)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_exported = true;
     if (is_particle_buffer(which)) {
-        DeviceGuard guard(sc->s.device);
-        CUDA_TRY(sync_reference_buffers(sc->s), "export");
+        Scene& s = sc->s;
+        DeviceGuard guard(s.device);
+        CUDA_TRY(ensure_reference(s, which), "export");
+        // a consumer that takes the pos/vel/density pointer reads it every
+        // frame: from now on every substep writes those three in place
+        if (s.engine == kEngineBinned && render_buffer(which) && !s.mirror) {
+            CUDA_TRY(sync_reference_buffers(s), "export");
+            s.mirror = true;
+        }
     }
     return MPM_OK;
 }
@@ -612,7 +633,14 @@ mpm_status mpm_get_ipc_handle(mpm_scene* sc, mpm_buffer which, void* handle, siz
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_exported = true;
     DeviceGuard guard(sc->s.device);
-    if (is_particle_buffer(which)) CUDA_TRY(sync_reference_buffers(sc->s), "export");
+    if (is_particle_buffer(which)) {
+        Scene& s = sc->s;
+        CUDA_TRY(ensure_reference(s, which), "export");
+        if (s.engine == kEngineBinned && render_buffer(which) && !s.mirror) {   // as mpm_get_buffer
+            CUDA_TRY(sync_reference_buffers(s), "export");
+            s.mirror = true;
+        }
+    }
     CUdeviceptr base = 0;
     size_t alloc = 0;
     CUDA_TRY(allocation_base(p, &base, &alloc), "allocation range");
@@ -632,7 +660,7 @@ mpm_status mpm_download(mpm_scene* sc, mpm_buffer which, void* host_dst, size_t 
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
     DeviceGuard guard(sc->s.device);
-    if (is_particle_buffer(which)) CUDA_TRY(sync_reference_buffers(sc->s), "export");
+    CUDA_TRY(ensure_reference(sc->s, which), "export");
     CUDA_TRY(cudaMemcpyAsync(host_dst, p, bytes, cudaMemcpyDeviceToHost, sc->s.stream), "download");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "download sync");
     return MPM_OK;
@@ -656,6 +684,8 @@ mpm_status mpm_upload(mpm_scene* sc, mpm_buffer which, const void* host_src, siz
         if (sc->s.engine == kEngineBinned) sc->s.fast_stale = true;
     }
     CUDA_TRY(cudaMemcpyAsync(p, host_src, bytes, cudaMemcpyHostToDevice, sc->s.stream), "upload");
+    // ADVECT reads only the slots the alive mask names: rebuild it from the new pool
+    if (which == MPM_BUF_DIFFUSE) CUDA_TRY(launch_alive_mask_build(sc->s), "alive mask");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "upload sync");
     return MPM_OK;
 }

@@ -497,11 +497,16 @@ __device__ __forceinline__ void reflect_axis(float& p, float& v, float lo, float
 __device__ __forceinline__ void diffuse_advect(mpm_diffuse_particle* __restrict__ pool, const float* __restrict__ mvf,
                                                const float4* __restrict__ vel4, const mpm_params& P,
                                                const mpm_advect_params& adv, const mpm_wall_params& W,
-                                               uint32_t* __restrict__ kill_bits, uint32_t* __restrict__ counts) {
+                                               uint32_t* __restrict__ kill_bits, uint32_t* __restrict__ counts,
+                                               uint32_t* __restrict__ alive_mask) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t M = adv.diffuse_max;
+    const uint32_t nwords = (M + 31u) / 32u;
+    // the warp's 32 slots are one mask word: a dead slot's record is never read
+    // (the reference tests pool[i].alive; the mask holds exactly those flags)
+    const uint32_t word = (i >> 5) < nwords ? alive_mask[i >> 5] : 0u;
     bool kill = false;
-    if (i < M && pool[i].alive != 0u) {
+    if (i < M && ((word >> (i & 31u)) & 1u)) {
         mpm_diffuse_particle p = pool[i];
         const f3 pos3 = mk(p.pos[0], p.pos[1], p.pos[2]);
         const float dt = P.dt, g = P.gravity;
@@ -562,7 +567,10 @@ __device__ __forceinline__ void diffuse_advect(mpm_diffuse_particle* __restrict_
     const unsigned b = __ballot_sync(0xffffffffu, kill);
     __shared__ uint32_t wc[kThreads / 32];
     if ((threadIdx.x & 31) == 0) {
-        if ((i >> 5) < (M + 31u) / 32u) kill_bits[i >> 5] = b;
+        if ((i >> 5) < nwords) {
+            kill_bits[i >> 5] = b;
+            if (b) alive_mask[i >> 5] = word & ~b;   // this warp owns the word
+        }
         wc[threadIdx.x >> 5] = __popc(b);
     }
     __syncthreads();
@@ -579,8 +587,9 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect(mpm_diffuse_particl
                                                               const float4* __restrict__ vel4, const mpm_params P,
                                                               const mpm_advect_params adv, const mpm_wall_params W,
                                                               uint32_t* __restrict__ kill_bits,
-                                                              uint32_t* __restrict__ counts) {
-    diffuse_advect(pool, mvf, vel4, P, adv, W, kill_bits, counts);
+                                                              uint32_t* __restrict__ counts,
+                                                              uint32_t* __restrict__ alive_mask) {
+    diffuse_advect(pool, mvf, vel4, P, adv, W, kill_bits, counts, alive_mask);
 }
 
 // ADVECT with the uniforms read from device memory (binned engine; graph-capturable).
@@ -590,8 +599,18 @@ __global__ void __launch_bounds__(kThreads) k_diffuse_advect_dev(mpm_diffuse_par
                                                                   const mpm_advect_params* __restrict__ adv,
                                                                   const mpm_wall_params* __restrict__ W,
                                                                   uint32_t* __restrict__ kill_bits,
-                                                                  uint32_t* __restrict__ counts) {
-    diffuse_advect(pool, nullptr, vel4, *P, *adv, *W, kill_bits, counts);
+                                                                  uint32_t* __restrict__ counts,
+                                                                  uint32_t* __restrict__ alive_mask) {
+    diffuse_advect(pool, nullptr, vel4, *P, *adv, *W, kill_bits, counts, alive_mask);
+}
+
+// Rebuilds the alive mask from the pool's alive flags (after the pool was
+// written from outside the diffuse passes).
+__global__ void __launch_bounds__(kThreads) k_alive_mask_build(const mpm_diffuse_particle* __restrict__ pool,
+                                                              uint32_t M, uint32_t* __restrict__ alive_mask) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned b = __ballot_sync(0xffffffffu, i < M && pool[i].alive != 0u);
+    if ((threadIdx.x & 31u) == 0 && (i >> 5) < (M + 31u) / 32u) alive_mask[i >> 5] = b;
 }
 
 // One free-list pass in a single launch: the exclusive scan of the group
@@ -620,7 +639,8 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_
                                                                 int mode, int32_t* __restrict__ top_hist,
                                                                 uint32_t* __restrict__ clear_bits, uint32_t nclear_bits,
                                                                 uint32_t* __restrict__ clear_counts,
-                                                                uint32_t nclear_counts) {
+                                                                uint32_t nclear_counts,
+                                                                uint32_t* __restrict__ alive_mask) {
     constexpr int kWarps = kPassThreads / 32;
     __shared__ uint32_t red[2][kWarps];
     __shared__ uint32_t excl[kPassThreads];
@@ -733,10 +753,12 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_freelist_pass(const uint32_
 #pragma unroll
                     for (uint32_t q = 0; q < kBatch; ++q) {
                         if (slot[jb + q] < M) {
-                            uint4* dst = reinterpret_cast<uint4*>(pool + slot[jb + q]);
+                            const uint32_t sl = slot[jb + q];
+                            uint4* dst = reinterpret_cast<uint4*>(pool + sl);
                             dst[0] = rec[q][0];
                             dst[1] = rec[q][1];
                             dst[2] = rec[q][2];
+                            atomicOr(&alive_mask[sl >> 5], 1u << (sl & 31u));   // staged records are alive
                         }
                     }
                 }
@@ -781,6 +803,13 @@ static inline void freelist_grid(uint32_t ng, uint32_t& B, uint32_t& R) {
     B = std::max(1u, blocks_for(ng, R));
 }
 
+cudaError_t launch_alive_mask_build(Scene& s) {
+    const DiffuseState& d = s.diffuse;
+    k_alive_mask_build<<<blocks_for(d.max_count, kThreads), kThreads, 0, s.stream>>>(d.pool, d.max_count, d.alive_mask);
+    s.launches++;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_apply_hand(Scene& s) {
     dim3 grid(blocks_for(s.hand_dims[0], 4), blocks_for(s.hand_dims[1], 4), blocks_for(s.hand_dims[2], 4));
     k_apply_hand<<<grid, dim3(4, 4, 4), 0, s.stream>>>(s.mvf, s.params, s.hand);
@@ -812,7 +841,7 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
         freelist_grid(ng, B, R);
         k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.spawn_bits, n, d.block_counts, ng, R, d.top, d.rank_state,
                                                     d.free_list, d.staging, d.pool, d.max_count, 0, nullptr, nullptr, 0,
-                                                    nullptr, 0);
+                                                    nullptr, 0, d.alive_mask);
         s.launches += 1;
     } else if (eval) {
         d.seed = d.seed + 1u;
@@ -825,15 +854,15 @@ cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const m
         Phase ph(s, MPM_PHASE_DIFFUSE_ADV);
         if (P_dev && W_dev && s.vel4)
             k_diffuse_advect_dev<<<mg, kThreads, 0, st>>>(d.pool, s.vel4, P_dev, d.adv_dev, W_dev, d.kill_bits,
-                                                          d.kill_counts);
+                                                          d.kill_counts, d.alive_mask);
         else
             k_diffuse_advect<<<mg, kThreads, 0, st>>>(d.pool, s.mvf, s.vel4, P, adv, s.walls, d.kill_bits,
-                                                      d.kill_counts);
+                                                      d.kill_counts, d.alive_mask);
         uint32_t B, R;
         freelist_grid(mg, B, R);
         k_freelist_pass<<<B, kPassThreads, 0, st>>>(d.kill_bits, M, d.kill_counts, mg, R, d.top, d.rank_state,
                                                     d.free_list, nullptr, d.pool, M, 1, d.top_hist, d.spawn_bits,
-                                                    (n + 31u) / 32u, d.block_counts, ng);
+                                                    (n + 31u) / 32u, d.block_counts, ng, nullptr);
         s.launches += 2;
         d.passes++;
         d.top_written = false;

@@ -13,6 +13,9 @@ cudaError_t launch_substep_plain(Scene& s);
 // APPLY_HAND over the scene's hand box (both engines).
 cudaError_t launch_apply_hand(Scene& s);
 
+// Rebuilds the diffuse alive mask from the pool (after the pool was uploaded).
+cudaError_t launch_alive_mask_build(Scene& s);
+
 // DiffuseGPU.step after G2P; eval = run the spawn-decision pass here.
 // P_dev / W_dev (binned engine): the scene's uniforms in device memory, read
 // by ADVECT instead of the host copies, so the launches can be captured in a

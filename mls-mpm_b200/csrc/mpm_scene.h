@@ -29,6 +29,11 @@ struct DiffuseState {
     // ranking scratch
     uint32_t* spawn_bits = nullptr;         // ceil(N/32) words, one bit per fluid particle id
     uint32_t* kill_bits = nullptr;          // ceil(M/32) words, one bit per slot
+    // one bit per pool slot, set exactly when the slot's record is alive: the
+    // spawn pass sets the bits of the slots it fills, ADVECT clears the bits
+    // of the slots it kills, and an upload of the pool rebuilds it; ADVECT
+    // reads only the records of set bits
+    uint32_t* alive_mask = nullptr;         // ceil(M/32) words
     uint32_t* block_counts = nullptr;       // spawners per group of kGroupIds fluid ids
     uint32_t* kill_counts = nullptr;        // kills per group of kGroupIds slots
     int32_t* rank_state = nullptr;          // [0] top before the pass, [1] total, [2] applied, [3] ticket, [4] kill passes
@@ -94,6 +99,10 @@ struct Scene {
     // binned engine: which copy of the particle state is newer
     bool ref_stale = false;    // reference-layout buffers behind the binned state
     bool fast_stale = false;   // binned state behind the reference-layout buffers
+    // binned engine: pos, vel and density in the reference layout are written
+    // by every substep (turned on by the first mpm_get_buffer of one of them,
+    // the sign of a consumer that reads them every frame)
+    bool mirror = false;
     uint64_t substeps_done = 0;
     uint64_t launches = 0;
 

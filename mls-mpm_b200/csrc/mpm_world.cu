@@ -670,29 +670,27 @@ __device__ __forceinline__ bool halo_cell(const ChunkHdr& h, const SceneDesc& sd
 // slot hb, written out through template indices (immediate offsets, no
 // per-cell control flow).  kClamp: encode with its clamp.
 template <bool kClamp, int K, int J, int I>
-__device__ __forceinline__ void mass_cell(const PW& w, float m, int32_t* a, uint32_t& sat) {
+__device__ __forceinline__ void mass_cell(const PW& w, float m, int32_t* a) {
     const float x = w.wx[I] * w.wy[J] * w.wz[K] * m;
-    const int32_t e = kClamp ? encode(x) : encode_unclamped(x);
-    if (kClamp) sat |= at_clamp(e);
-    atomicAdd(a + (K * kHXY + J * kHX + I), e);
+    atomicAdd(a + (K * kHXY + J * kHX + I), kClamp ? encode(x) : encode_unclamped(x));
 }
 template <bool kClamp, int K, int J>
-__device__ __forceinline__ void mass_row(const PW& w, float m, int32_t* a, uint32_t& sat) {
-    mass_cell<kClamp, K, J, 0>(w, m, a, sat);
-    mass_cell<kClamp, K, J, 1>(w, m, a, sat);
-    mass_cell<kClamp, K, J, 2>(w, m, a, sat);
+__device__ __forceinline__ void mass_row(const PW& w, float m, int32_t* a) {
+    mass_cell<kClamp, K, J, 0>(w, m, a);
+    mass_cell<kClamp, K, J, 1>(w, m, a);
+    mass_cell<kClamp, K, J, 2>(w, m, a);
 }
 template <bool kClamp>
-__device__ __forceinline__ void mass_contrib_shared(const PW& w, float m, int32_t* a, uint32_t& sat) {
-    mass_row<kClamp, 0, 0>(w, m, a, sat);
-    mass_row<kClamp, 0, 1>(w, m, a, sat);
-    mass_row<kClamp, 0, 2>(w, m, a, sat);
-    mass_row<kClamp, 1, 0>(w, m, a, sat);
-    mass_row<kClamp, 1, 1>(w, m, a, sat);
-    mass_row<kClamp, 1, 2>(w, m, a, sat);
-    mass_row<kClamp, 2, 0>(w, m, a, sat);
-    mass_row<kClamp, 2, 1>(w, m, a, sat);
-    mass_row<kClamp, 2, 2>(w, m, a, sat);
+__device__ __forceinline__ void mass_contrib_shared(const PW& w, float m, int32_t* a) {
+    mass_row<kClamp, 0, 0>(w, m, a);
+    mass_row<kClamp, 0, 1>(w, m, a);
+    mass_row<kClamp, 0, 2>(w, m, a);
+    mass_row<kClamp, 1, 0>(w, m, a);
+    mass_row<kClamp, 1, 1>(w, m, a);
+    mass_row<kClamp, 1, 2>(w, m, a);
+    mass_row<kClamp, 2, 0>(w, m, a);
+    mass_row<kClamp, 2, 1>(w, m, a);
+    mass_row<kClamp, 2, 2>(w, m, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -715,7 +713,6 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     // the accumulators start at zero and every flush zeroes what it read
     for (int i = threadIdx.x; i < kHaloCells; i += blockDim.x) acc[i] = 0;
     __syncthreads();
-    uint32_t sat = 0;   // a contribution of this thread's particles hit encode's clamp in this chunk
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         const ChunkHdr h = hs;
         const uint32_t nxt = ch + gridDim.x;
@@ -746,9 +743,17 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             if (fast) {
                 // weight <= 0.4219: for |mass| < 47000 encode's clamp is the identity
                 const bool safe = fabsf(q[r].w) < 47000.0f;
-                if (safe) mass_contrib_shared<false>(w, q[r].w, acc + hb, sat);
-                else mass_contrib_shared<true>(w, q[r].w, acc + hb, sat);
+                if (safe) {
+                    mass_contrib_shared<false>(w, q[r].w, acc + hb);
+                } else {
+                    // health: encode's clamp may engage (a weight times |mass| >= 20000 needs |mass| >= 47000)
+                    atomicOr(&v.health[h.scene], MPM_HEALTH_SATURATED);
+                    mass_contrib_shared<true>(w, q[r].w, acc + hb);
+                }
             } else if (valid) {
+                // health: every position that is NaN or infinite takes this path
+                // (its cell is 0 or saturated, outside every halo); it never heals
+                if (!(fabsf(q[r].x + q[r].y + q[r].z) <= 3.0e38f)) atomicOr(&v.health[h.scene], MPM_HEALTH_NONFINITE);
                 // stencil outside the halo or the grid: bounds-checked global atomics
                 const int32_t X = sd.X, Y = sd.Y, Z = sd.Z;
                 int32_t* scm = cm + sd.cell_base;
@@ -759,13 +764,12 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
                             if (xx < 0 || xx >= X || yy < 0 || yy >= Y || zz < 0 || zz >= Z) continue;
                             const float ww = w.wx[i] * w.wy[j] * w.wz[kk];
                             const int32_t e = encode(ww * q[r].w);
-                            sat |= at_clamp(e);
+                            if (at_clamp(e)) atomicOr(&v.health[h.scene], MPM_HEALTH_SATURATED);
                             atomicAdd(&scm[(zz * Y + yy) * X + xx], e);
                         }
             }
         }
-        if (__syncthreads_or((int)sat) && threadIdx.x == 0) atomicOr(&v.health[h.scene], MPM_HEALTH_SATURATED);
-        sat = 0;
+        __syncthreads();
         // every thread holds this chunk's header: the next one can replace it
         if (threadIdx.x == 0 && nxt < nch) chunk_header_from(nci, nlast, ngeo, hs);
         int32_t* scm = cm + sd.cell_base;
@@ -973,7 +977,7 @@ struct MomTerms {
 template <bool kClamp, int K, int J, int I>
 __device__ __forceinline__ void mom_cell(const PW& w, const MomIn& in, const MomTerms& t, float qx, float qy,
                                          float qzz, float gx, float gy, float gz, int32_t* a0, int32_t* a1,
-                                         int32_t* a2, uint32_t& sat) {
+                                         int32_t* a2) {
     const float ww = w.wx[I] * (w.wy[J] * w.wz[K]);
     const float Qx = qx + t.qz[0][K];
     const float Qy = qy + t.qz[1][K];
@@ -985,18 +989,14 @@ __device__ __forceinline__ void mom_cell(const PW& w, const MomIn& in, const Mom
     const float vy = ww * (in.m * (in.vy + Qy) + fyf);
     const float vz = ww * (in.m * (in.vz + Qz) + fzf);
     constexpr int o = K * kHXY + J * kHX + I;
-    const int32_t ex = kClamp ? encode(vx) : encode_unclamped(vx);
-    const int32_t ey = kClamp ? encode(vy) : encode_unclamped(vy);
-    const int32_t ez = kClamp ? encode(vz) : encode_unclamped(vz);
-    if (kClamp) sat |= at_clamp(ex) | at_clamp(ey) | at_clamp(ez);
-    atomicAdd(a0 + o, ex);
-    atomicAdd(a1 + o, ey);
-    atomicAdd(a2 + o, ez);
+    atomicAdd(a0 + o, kClamp ? encode(vx) : encode_unclamped(vx));
+    atomicAdd(a1 + o, kClamp ? encode(vy) : encode_unclamped(vy));
+    atomicAdd(a2 + o, kClamp ? encode(vz) : encode_unclamped(vz));
 }
 
 template <bool kClamp, int J, int I>
 __device__ __forceinline__ void mom_column(const PW& w, const MomIn& in, const MomTerms& t, int32_t* a0,
-                                           int32_t* a1, int32_t* a2, uint32_t& sat) {
+                                           int32_t* a1, int32_t* a2) {
     const float dxi = t.dxs[I], dyj = t.dys[J];
     const float qx = in.a00 * dxi + in.a01 * dyj;
     const float qy = in.a10 * dxi + in.a11 * dyj;
@@ -1004,14 +1004,14 @@ __device__ __forceinline__ void mom_column(const PW& w, const MomIn& in, const M
     const float gx = t.s00 * dxi + t.s01 * dyj;
     const float gy = t.s01 * dxi + t.s11 * dyj;
     const float gz = t.s02 * dxi + t.s12 * dyj;
-    mom_cell<kClamp, 0, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2, sat);
-    mom_cell<kClamp, 1, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2, sat);
-    mom_cell<kClamp, 2, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2, sat);
+    mom_cell<kClamp, 0, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
+    mom_cell<kClamp, 1, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
+    mom_cell<kClamp, 2, J, I>(w, in, t, qx, qy, qzz, gx, gy, gz, a0, a1, a2);
 }
 
 template <bool kClamp>
 __device__ __forceinline__ void mom_contrib_shared(const PW& w, const MomIn& in, const float* s, float coef,
-                                                   int32_t (*acc)[kHaloCells], int hb, uint32_t& sat) {
+                                                   int32_t (*acc)[kHaloCells], int hb) {
     MomTerms t;
     t.s00 = s[0]; t.s11 = s[1]; t.s01 = s[3]; t.s02 = s[4]; t.s12 = s[5];
     const float s22 = s[2];
@@ -1031,15 +1031,15 @@ __device__ __forceinline__ void mom_contrib_shared(const PW& w, const MomIn& in,
     int32_t* a0 = &acc[0][hb];
     int32_t* a1 = &acc[1][hb];
     int32_t* a2 = &acc[2][hb];
-    mom_column<kClamp, 0, 0>(w, in, t, a0, a1, a2, sat);
-    mom_column<kClamp, 0, 1>(w, in, t, a0, a1, a2, sat);
-    mom_column<kClamp, 0, 2>(w, in, t, a0, a1, a2, sat);
-    mom_column<kClamp, 1, 0>(w, in, t, a0, a1, a2, sat);
-    mom_column<kClamp, 1, 1>(w, in, t, a0, a1, a2, sat);
-    mom_column<kClamp, 1, 2>(w, in, t, a0, a1, a2, sat);
-    mom_column<kClamp, 2, 0>(w, in, t, a0, a1, a2, sat);
-    mom_column<kClamp, 2, 1>(w, in, t, a0, a1, a2, sat);
-    mom_column<kClamp, 2, 2>(w, in, t, a0, a1, a2, sat);
+    mom_column<kClamp, 0, 0>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 0, 1>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 0, 2>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 1, 0>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 1, 1>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 1, 2>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 2, 0>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 2, 1>(w, in, t, a0, a1, a2);
+    mom_column<kClamp, 2, 2>(w, in, t, a0, a1, a2);
 }
 
 // Density of one particle from the staged halo masses (shaders.js:305-313):
@@ -1074,7 +1074,7 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
                                              uint32_t p, const float4 pm, const float4 vi, const float* a,
                                              const float* mh, int32_t (*acc)[kHaloCells],
                                              const float* __restrict__ scmf, int32_t* __restrict__ smv,
-                                             float* __restrict__ dens, uint32_t& sat) {
+                                             float* __restrict__ dens, uint32_t* __restrict__ health) {
     const uint32_t X = sd.X, SLICE = sd.X * sd.Y, G = sd.G;
     const PW w = particle_weights(pm.x, pm.y, pm.z);
     const bool fast = valid && in_halo(w, h, sd);
@@ -1121,12 +1121,13 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
     const float bz = am * (fabsf(in.vz) + 1.5f * (fabsf(in.a20) + fabsf(in.a21) + fabsf(in.a22))) +
                      ac * 1.5f * (fabsf(s[4]) + fabsf(s[5]) + fabsf(s[2]));
     const bool safe = fmaxf(bx, fmaxf(by, bz)) * 0.4222f < 19000.0f;
+    // health: the bound says encode's clamp may engage (a contribution may reach 20000)
+    if (live && !safe) atomicOr(health, MPM_HEALTH_SATURATED);
     if (live && fast) {
-        if (safe) mom_contrib_shared<false>(w, in, s, coef, acc, hb, sat);
-        else mom_contrib_shared<true>(w, in, s, coef, acc, hb, sat);
+        if (safe) mom_contrib_shared<false>(w, in, s, coef, acc, hb);
+        else mom_contrib_shared<true>(w, in, s, coef, acc, hb);
     } else if (live) {
         auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
-            sat |= at_clamp(ex) | at_clamp(ey) | at_clamp(ez);
             const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
             if (cidx < G) {
                 atomicAdd(smv + 3ull * cidx + 0, ex);
@@ -1213,7 +1214,6 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
     cp_async_wait();
     __syncthreads();
     int b = 0;
-    uint32_t sat = 0;   // a contribution of this thread's particles hit encode's clamp in this chunk
     for (uint32_t ch = blockIdx.x; ch < nch; ch += G) {
         const ChunkHdr h = hdr[b];
         const uint32_t nxt = ch + G, nxt2 = nxt + G;
@@ -1245,7 +1245,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
             float4 pmn = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vin = pmn;
             float an[9];
             mom_load(v, pn, vn, posm, velid, aff, plane, pmn, vin, an);
-            mom_particle(v, h, sd, valid, p, pm, vi, a, mh[b], acc, scmf, smv, dens, sat);
+            mom_particle(v, h, sd, valid, p, pm, vi, a, mh[b], acc, scmf, smv, dens, v.health + h.scene);
             p = pn;
             valid = vn;
             pm = pmn;
@@ -1253,8 +1253,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
 #pragma unroll
             for (int e = 0; e < 9; ++e) a[e] = an[e];
         }
-        if (__syncthreads_or((int)sat) && threadIdx.x == 0) atomicOr(&v.health[h.scene], MPM_HEALTH_SATURATED);
-        sat = 0;
+        __syncthreads();
         // hdr[b] is free: the header two chunks ahead goes there
         if (threadIdx.x == 0 && nxt2 < nch) hdr[b] = unpack_header(nh0, nh1);
         const int hn = halo_span(h);
@@ -1498,18 +1497,21 @@ struct G2POut {
 // so the atomic's round trip overlaps later work).
 __device__ __forceinline__ uint32_t g2p_store(const G2POut& o, const SceneDesc& sd, uint32_t p, const float4 q,
                                               const float4 vi, float density, float gvx, float gvy, float gvz,
-                                              const float* B, uint32_t& bad) {
+                                              const float* B, const RefOut& ro, bool mirror) {
 #pragma unroll
     for (int e = 0; e < 9; ++e) o.aff[e * o.plane + p] = B[e] * 4.0f;
     f3 np, nv;
     g2p_finish(q, gvx, gvy, gvz, sd.P, sd.W, np, nv);
-    // health: a NaN or an infinity in the new state shows in the sum (positions
-    // are clamped to the grid and velocities stay below ~1e10, so a finite
-    // state cannot overflow it)
-    const float hs = ((np.x + np.y) + (np.z + nv.x)) + (nv.y + nv.z);
-    bad |= !(fabsf(hs) <= 3.0e38f) ? 1u : 0u;
     o.posm[p] = make_float4(np.x, np.y, np.z, q.w);
     o.velid[p] = make_float4(nv.x, nv.y, nv.z, vi.w);
+    if (mirror) {   // particle_pos/vel (shaders.js:703-704) and particle_density (shaders.js:314) by id
+        const uint32_t id = __float_as_uint(vi.w) - sd.id_base;
+        if (id < sd.n) {
+            ro.pos[id] = make_float4(np.x, np.y, np.z, 0.0f);
+            ro.vel[id] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+            ro.dens[id] = density;
+        }
+    }
     // binning of the new position
     int32_t cx, cy, cz;
     bin_cell(sd, np.x, np.y, np.z, cx, cy, cz);
@@ -1539,15 +1541,13 @@ __device__ __forceinline__ uint32_t g2p_store(const G2POut& o, const SceneDesc& 
 
 // G2P of a particle whose stencil leaves the halo box or the grid (rare): the
 // reference's linear stencil index with a bounds guard, then the epilogue.
-// Returns 1 when the new state is not finite.
-__device__ __noinline__ uint32_t g2p_direct_particle(const G2POut o, const SceneDesc* sdp, uint32_t p, const float4 q,
-                                                     const float4 vi, const float4* __restrict__ vel4) {
+__device__ __noinline__ void g2p_direct_particle(const G2POut o, const SceneDesc* sdp, uint32_t p, const float4 q,
+                                                 const float4 vi, const float4* __restrict__ vel4, const RefOut ro,
+                                                 bool mirror) {
     const SceneDesc& sd = *sdp;
     const PW w = particle_weights(q.x, q.y, q.z);
     const G2PSum r = g2p_gather_direct(w, q, vel4, sd.X, sd.Y, sd.G);
-    uint32_t bad = 0;
-    o.rank[p] = g2p_store(o, sd, p, q, vi, o.dens[p], r.gv[0], r.gv[1], r.gv[2], r.B, bad);
-    return bad;
+    o.rank[p] = g2p_store(o, sd, p, q, vi, o.dens[p], r.gv[0], r.gv[1], r.gv[2], r.B, ro, mirror);
 }
 
 template <uint32_t kC>
@@ -1557,7 +1557,8 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
                                                               const float* __restrict__ cmf,
                                                               float4* __restrict__ posm_out,
                                                               float4* __restrict__ velid_out,
-                                                              float* __restrict__ aff_out, DiffuseView dv) {
+                                                              float* __restrict__ aff_out, DiffuseView dv,
+                                                              RefOut ro) {
     constexpr int kPer = kC / kChunkThreads;
     __shared__ float4 vh[kHaloCells];   // staged grid velocities (x, y, z, 0)
     __shared__ uint4 nhs[2];              // the next chunk's header words
@@ -1568,7 +1569,6 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     uint32_t cached = kHole;
     // rank of the last particle whose atomic is still in flight
     uint32_t pend_p = kHole, pend_rank = 0;
-    uint32_t bad = 0;   // this thread saw a non-finite new state in the current chunk
     const float bubble_min = dv.enabled ? dv.gen->density_bubble_min : 0.0f;
     const float pressure_threshold = dv.enabled ? dv.gen->pressure_threshold : 0.0f;
     const float ke_threshold = dv.enabled ? dv.gen->ke_threshold : 0.0f;
@@ -1622,6 +1622,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
             hs = unpack_header(nhs[0], nhs[1]);
         }
         const bool spawn_scene = dv.enabled && h.scene == dv.scene;
+        const bool mirror = ro.enabled && h.scene == ro.scene;
         const G2POut out{posm_out, velid_out, aff_out, plane, v.key, v.rank, v.cell_count, v.tile_flags, v.dens,
                          cmf + sd.cell_base, spawn_scene ? dv.gen : nullptr, bubble_min, pressure_threshold,
                          ke_threshold, dv.staging, dv.spawn_bits, dv.group_counts};
@@ -1633,7 +1634,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
             const float4 vi = make_float4(0.0f, 0.0f, 0.0f, ids[r]);
             const PW w = particle_weights(q.x, q.y, q.z);
             if (!in_halo(w, h, sd)) {
-                bad |= g2p_direct_particle(out, &sd, p, q, vi, svel);
+                g2p_direct_particle(out, &sd, p, q, vi, svel, ro, mirror);
                 continue;
             }
             float gvx = 0.0f, gvy = 0.0f, gvz = 0.0f;
@@ -1663,15 +1664,13 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
                     }
                 }
             }
-            const uint32_t rk = g2p_store(out, sd, p, q, vi, dns[r], gvx, gvy, gvz, B, bad);
+            const uint32_t rk = g2p_store(out, sd, p, q, vi, dns[r], gvx, gvy, gvz, B, ro, mirror);
             // the previous particle's rank: its atomic has long returned
             if (pend_p != kHole) v.rank[pend_p] = pend_rank;
             pend_p = p;
             pend_rank = rk;
         }
-        // the chunk's scene is flagged once if any of its particles went non-finite
-        if (__syncthreads_or((int)bad) && threadIdx.x == 0) atomicOr(&v.health[h.scene], MPM_HEALTH_NONFINITE);
-        bad = 0;
+        __syncthreads();
     }
     if (pend_p != kHole) v.rank[pend_p] = pend_rank;
 }
@@ -2018,8 +2017,11 @@ cudaError_t world_export_scene(World& w, int slot, float4* pos, float4* vel, flo
     return cudaGetLastError();
 }
 
-// Enqueues one substep of all scenes on w.stream (capturable when ds is null).
-static cudaError_t enqueue_substep(World& w, Scene* ds) {
+// Enqueues one substep of all scenes on w.stream.  ds: the single-scene owner
+// (its diffuse update runs when enabled, its profiler times the phases; null
+// in a graph capture without diffuse, and for batches); ro: the owner's
+// reference-layout mirrors.
+static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro) {
     const WorldView v = w.view();
     cudaStream_t st = w.stream;
     const int cur = w.cur, nxt = cur ^ 1;
@@ -2102,11 +2104,11 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
         if (w.chunk == kChunkSmall)
             k_g2p_chunks<kChunkSmall><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4,
                                                                              w.cmf, w.posm[nxt], w.velid[nxt],
-                                                                             w.aff[nxt], dv);
+                                                                             w.aff[nxt], dv, ro);
         else
             k_g2p_chunks<kChunk><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4,
                                                                         w.cmf, w.posm[nxt], w.velid[nxt],
-                                                                        w.aff[nxt], dv);
+                                                                        w.aff[nxt], dv, ro);
         w.launches++;
     }
     w.cur = nxt;
@@ -2126,6 +2128,14 @@ static cudaError_t enqueue_substep(World& w, Scene* ds) {
 }
 
 cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
+    RefOut ro{};
+    if (ds && ds->mirror && ds->world_slot >= 0) {
+        ro.enabled = 1;
+        ro.scene = (uint32_t)ds->world_slot;
+        ro.pos = ds->pos;
+        ro.vel = ds->vel;
+        ro.dens = ds->dens;
+    }
     // chunk size: one pass per chunk when full-size chunks would leave blocks
     // of the chunk kernels idle (a new size means new captured graphs)
     const uint32_t chunk = (uint64_t)w.n_total < (uint64_t)w.item_blocks * kChunk ? kChunkSmall : kChunk;
@@ -2138,12 +2148,14 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
     const bool diffuse = ds && ds->diffuse.enabled;
     const bool profiling = ds && ds->profile;
     // a substep that must recount runs eagerly; the captured graphs never count
-    if (!use_graph || profiling || !w.counted) return enqueue_substep(w, ds);
+    if (!use_graph || profiling || !w.counted) return enqueue_substep(w, ds, ro);
     // the diffuse update joins the graph: its kernels read the uniforms from
     // the device scene table and the advect parameters from a device copy
     Scene* dsc = diffuse ? ds : nullptr;
     const int p = w.cur;   // cur and gbuf flip together: one graph per parity
-    if (!w.graph[p] || w.graph_gen[p] != w.generation || w.graph_diffuse[p] != diffuse) {
+    const bool mirror = ro.enabled != 0;
+    if (!w.graph[p] || w.graph_gen[p] != w.generation || w.graph_diffuse[p] != diffuse ||
+        w.graph_mirror[p] != mirror) {
         if (w.graph[p]) {
             cudaGraphExecDestroy(w.graph[p]);
             w.graph[p] = nullptr;
@@ -2158,7 +2170,7 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
         cudaGraph_t g = nullptr;
         e = cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;
-        const cudaError_t e2 = enqueue_substep(w, dsc);
+        const cudaError_t e2 = enqueue_substep(w, dsc, ro);
         e = cudaStreamEndCapture(w.stream, &g);
         if (e2 != cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaGraphInstantiate(&w.graph[p], g, 0);
@@ -2181,6 +2193,7 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
         }
         w.graph_gen[p] = w.generation;
         w.graph_diffuse[p] = diffuse;
+        w.graph_mirror[p] = mirror;
     }
     e = cudaGraphLaunch(w.graph[p], w.stream);
     if (e != cudaSuccess) return e;

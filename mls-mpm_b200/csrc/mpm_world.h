@@ -114,6 +114,18 @@ struct DiffuseView {
     uint32_t* group_counts;          // spawners per group of kGroupIds ids
 };
 
+// Reference-layout particle buffers (by particle id) that the substep keeps
+// current for the one scene of a single-scene world whose consumer reads them
+// every frame (a renderer's vertex inputs): G2P writes pos/vel, P2G_MOM
+// writes density.  Disabled: nothing written.
+struct RefOut {
+    int enabled;
+    uint32_t scene;
+    float4* pos;
+    float4* vel;
+    float* dens;
+};
+
 // Host record of a scene in a world.
 struct SceneRec {
     bool live = false;
@@ -207,6 +219,7 @@ struct World {
     uint64_t graph_gen[2] = {0, 0};
     uint64_t graph_kernels[2] = {0, 0};     // kernels in each graph (launch accounting)
     bool graph_diffuse[2] = {false, false};  // the graph includes the diffuse update of its scene
+    bool graph_mirror[2] = {false, false};   // the graph writes the owner's reference-layout mirrors
 
     WorldView view() const;
 };
@@ -238,10 +251,10 @@ void world_set_uniforms(World& w, int slot, const mpm_params& P, const mpm_wall_
                         const mpm_hand_params* H, int hand_active, const int32_t* hand_dims);
 
 struct Scene;
-// One substep of every scene.  diffuse_owner: the single-scene wrapper whose
-// diffuse pool follows scene slot 0 (null: no diffuse).  use_graph: replay a
-// captured CUDA graph of the substep (captured on first use and whenever the
-// scene set changes).
-cudaError_t world_substep(World& w, Scene* diffuse_owner, bool use_graph);
+// One substep of every scene.  owner: the single-scene wrapper of a world of
+// one scene (its diffuse pool and reference-layout mirrors follow that scene;
+// null for batches).  use_graph: replay a captured CUDA graph of the substep
+// (captured on first use and whenever the scene set changes).
+cudaError_t world_substep(World& w, Scene* owner, bool use_graph);
 
 }  // namespace mpm
