@@ -7,6 +7,8 @@ Workload (one "step" = one substep of the scene, all passes incl. diffuse):
 Multi-GPU (torchrun): every rank simulates its own independent scene (seed =
 rank) — scene sharding with no data-path collective; `value` sums all ranks'
 particle-updates over the max-over-ranks device time ("scaling": "weak").
+The batched and served comparisons shard their scene mix and job stream over
+the ranks (mls_mpm_b200.shard), one batch or serving loop per GPU.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -251,25 +253,36 @@ def main():
     # reference's frame drives it (main.js:504-528): per step the host moves
     # the hand (fluid-gpu.js:479-527; a small cylinder sweeping the empty top
     # corner of the domain, so every frame carries new uniforms, uploaded from
-    # pinned memory), steps the scene, queues the diffuse alive-count readback
-    # (diffuse-gpu.js:172-176) and polls it (178-188) without waiting; the
-    # clock stops after the last readback has landed.
-    fl = make()
-    X, Y, Z = scene.grid
-    barrier()
-    t0 = time.perf_counter()
-    for s in range(args.steps):
-        hz = Z - 14.0 + 2.0 * math.sin(0.1 * s)
-        fl.updateHand([X - 14.0, Y - 12.0, hz], [0.0, 0.0, 0.5], 3.0, 0.2, True, [X - 14.0, Y - 12.0, Z + 40.0])
-        fl.simFrame()
+    # pinned memory), steps the scene, takes the particle position, velocity
+    # and density buffers the renderer draws from (fluid-renderer.js:315-328;
+    # zero-copy device pointers in the reference layout), queues the diffuse
+    # alive-count readback (diffuse-gpu.js:172-176) and polls it (178-188)
+    # without waiting; the clock stops after the last readback has landed.
+    # The same loop without the render buffers is reported beside it.
+    def e2e_run(render):
+        fl = make()
+        X, Y, Z = scene.grid
+        barrier()
+        t0 = time.perf_counter()
+        for s in range(args.steps):
+            hz = Z - 14.0 + 2.0 * math.sin(0.1 * s)
+            fl.updateHand([X - 14.0, Y - 12.0, hz], [0.0, 0.0, 0.5], 3.0, 0.2, True, [X - 14.0, Y - 12.0, Z + 40.0])
+            fl.simFrame()
+            if render:
+                for name in ("pos", "vel", "density"):
+                    fl.get_buffer(name)
+            if fl.diffuse is not None:
+                fl.diffuse.requestDebugReadback()
+                fl.diffuse.pollDebug()
+        fl.sync()
         if fl.diffuse is not None:
-            fl.diffuse.requestDebugReadback()
             fl.diffuse.pollDebug()
-    fl.sync()
-    if fl.diffuse is not None:
-        fl.diffuse.pollDebug()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    fl.destroy()
+        secs = max_over_ranks(time.perf_counter() - t0)
+        fl.destroy()
+        return secs
+
+    e2e_s = e2e_run(render=True)
+    e2e_plain_s = e2e_run(render=False)
 
     # (3) per-phase device time over the same substeps (CUDA events on the scene stream),
     # after the end-to-end run so that both timed loops follow each other
@@ -323,16 +336,18 @@ def main():
                                  "frac": sub_bytes / (sub_ms * 1e-3) / 1e9 / peak,
                                  "algorithmic_bytes": sub_bytes, "note": "180 B/particle + 60 B/cell"},
             "phase_ms": phase_ms,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "render_buffers": "particle pos, vel and density taken every frame (reference layout, device)",
+                    "without_render_buffers": total_updates / e2e_plain_s},
             "gpu_launches": n_launch,
             "clocks": clocks.summary()}
 
     if rank == 0 and not args.no_drift:
         line["drift_f32_vs_f64"] = drift_report(local)
     if not args.no_batched:
-        line["batched"] = batched_comparison(local)
+        line["batched"] = batched_comparison(local, ws=ws, rank=rank, reduce_max=max_over_ranks)
     if not args.no_served:
-        line["served"] = served_comparison(local)
+        line["served"] = served_comparison(local, ws=ws, rank=rank)
 
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -381,25 +396,32 @@ def drift_report(local, substeps=100, checkpoints=(1, 10, 100), threads=None):
             "note": "GPU f32 state is bit-identical to the f32 oracle at every substep", "checkpoints": rows}
 
 
-def batched_comparison(local, substeps=200, warmup=20, count=64, seed=0):
+def batched_comparison(local, substeps=200, warmup=20, count=64, seed=0, ws=1, rank=0, reduce_max=None):
     """The batched workload (scenes.batch_mix: 64 scenes, 200 substeps) run as
     one batch (one launch per kernel per substep for all scenes, CUDA graph,
     autotuned launch shape) and one scene at a time through the single-scene
     path (the same kernels, each scene's `substeps` substeps in turn on its own
     stream).  Both are device-timed with CUDA events after `warmup` substeps
-    (the autotuner's trials fall in the batch's warm-up)."""
+    (the autotuner's trials fall in the batch's warm-up).  With ws ranks each
+    rank runs its share of the scenes (shard.assign on particle-updates) in
+    both arms; times are the max over ranks."""
     import torch
-    from mls_mpm_b200 import abi, scenes
+    from mls_mpm_b200 import abi, scenes, shard
     from mls_mpm_b200.abi import check
     from mls_mpm_b200.batch import Batch, default_params
     from mls_mpm_b200.fluid_gpu import FluidGPU
 
-    mix = scenes.batch_mix(count, seed)
+    reduce_max = reduce_max or (lambda x: x)
+    full = scenes.batch_mix(count, seed)
+    n_all = sum(s.n for s in full)
+    cells_all = sum(s.cells for s in full)
+    mine = shard.my_items([shard.scene_cost(s, substeps) for s in full], ws, rank)
+    mix = [full[i] for i in mine]
     n_tot = sum(s.n for s in mix)
     cells = sum(s.cells for s in mix)
     dev = torch.device("cuda", local)
     # batched
-    b = Batch(n_tot, cells, count, device=local, flags=abi.BATCH_AUTOTUNE)
+    b = Batch(max(1, n_tot), max(1, cells), max(1, len(mix)), device=local, flags=abi.BATCH_AUTOTUNE)
     for s in mix:
         b.add(default_params(s.grid, s.n, b.lib), s.pos, s.mass, s.vel, s.affine)
     b.step(warmup)
@@ -411,7 +433,7 @@ def batched_comparison(local, substeps=200, warmup=20, count=64, seed=0):
     b.step(substeps)
     e1.record(st)
     e1.synchronize()
-    batched_ms = e0.elapsed_time(e1)
+    batched_ms = reduce_max(e0.elapsed_time(e1))
     info = b.info()
     launches = info.launches - l0
     shape = (info.item_blocks, info.grid_blocks)
@@ -438,10 +460,13 @@ def batched_comparison(local, substeps=200, warmup=20, count=64, seed=0):
         lib.mpm_launch_count(h, ctypes.byref(c1))
         alone_launches += c1.value - c0.value
         fl.destroy()
-    updates = n_tot * substeps
-    sub_bytes = 180 * n_tot + 60 * cells
+    alone_ms = reduce_max(alone_ms)
+    updates = n_all * substeps
+    sub_bytes = 180 * n_all + 60 * cells_all
     peak, _ = measured_peaks()
-    return {"workload": f"batch_mix: {count} scenes, {n_tot} particles, {cells} cells, seed {seed}",
+    peak *= ws
+    return {"workload": f"batch_mix: {count} scenes, {n_all} particles, {cells_all} cells, seed {seed}"
+                        + (f"; scene-sharded over {ws} GPUs (max over ranks)" if ws > 1 else ""),
             "substeps": substeps, "warmup": warmup,
             "batched": {"value": updates / (batched_ms / 1e3), "unit": UNIT, "ms_per_substep": batched_ms / substeps,
                         "gpu_launches": launches, "launch_shape": {"item_blocks": shape[0], "grid_blocks": shape[1]},
@@ -451,29 +476,35 @@ def batched_comparison(local, substeps=200, warmup=20, count=64, seed=0):
             "speedup": alone_ms / batched_ms}
 
 
-def served_comparison(local, rates=(50.0, 200.0, 2000.0), count=64, seed=0, budget_gb=150.0):
+def served_comparison(local, rates=(50.0, 200.0, 2000.0), count=64, seed=0, budget_gb=150.0, ws=1, rank=0):
     """The served workload: `count` jobs (scenes.serve_job) arriving as a
     Poisson stream at each rate, run by the serving loop (admission against an
     HBM budget, resident scenes batched every substep) and by the plain
     per-job path (one job at a time in arrival order through the single-scene
     path).  Plain-path latencies come from each job's device-timed service
-    time played through the same arrival times in FIFO order."""
+    time played through the same arrival times in FIFO order.  With ws ranks
+    each rank serves its share of the stream (shard.assign on
+    particle-updates, arrival times kept); throughput is all ranks' updates
+    over the slowest rank's wall time, latencies are pooled."""
     import torch
-    from mls_mpm_b200 import abi, scenes
+    from mls_mpm_b200 import abi, scenes, shard
     from mls_mpm_b200.abi import check
     from mls_mpm_b200.batch import default_params
     from mls_mpm_b200.fluid_gpu import FluidGPU
     from mls_mpm_b200.server import Server
 
-    jobs = [scenes.serve_job(seed, i) for i in range(count)]
-    updates = sum(sc.n * k for sc, k in jobs)
+    all_jobs = [scenes.serve_job(seed, i) for i in range(count)]
+    mine = shard.shard_jobs(all_jobs, ws, rank)
+    jobs = [all_jobs[i] for i in mine]
+    updates_all = sum(sc.n * k for sc, k in all_jobs)
     dev = torch.device("cuda", local)
     free, _ = torch.cuda.mem_get_info(dev)
     budget = int(min(budget_gb * 1e9, free - 12e9))
-    cpp = max(sc.cells / sc.n for sc, _ in jobs)
-    out = {"workload": f"serve_job x{count}: {sum(sc.n for sc, _ in jobs)} particles, "
-                       f"{updates} particle-updates, seed {seed}",
-           "budget_bytes": budget, "budget_note": f"min({budget_gb:g} GB, free device memory - 12 GB)",
+    cpp = max(sc.cells / sc.n for sc, _ in all_jobs)
+    out = {"workload": f"serve_job x{count}: {sum(sc.n for sc, _ in all_jobs)} particles, "
+                       f"{updates_all} particle-updates, seed {seed}"
+                       + (f"; job stream sharded over {ws} GPUs" if ws > 1 else ""),
+           "budget_bytes": budget, "budget_note": f"min({budget_gb:g} GB, free device memory - 12 GB) per GPU",
            "rates": {}}
     # plain per-job path: service time of each job alone (device-timed)
     service = []
@@ -493,25 +524,40 @@ def served_comparison(local, rates=(50.0, 200.0, 2000.0), count=64, seed=0, budg
     srv = Server(budget, scene_capacity=max(64, count), cells_per_particle=cpp, device=local)
     try:
         for rate in rates:
-            arr = scenes.poisson_arrivals(rate, count, seed)
-            for (sc, k), t in zip(jobs, arr):
-                srv.submit(default_params(sc.grid, sc.n, srv.lib), sc.pos, sc.mass, k, float(t), vel4=sc.vel)
+            arr_all = scenes.poisson_arrivals(rate, count, seed)
+            arr = [float(arr_all[i]) for i in mine]
+            ids = [srv.submit(default_params(sc.grid, sc.n, srv.lib), sc.pos, sc.mass, k, t, vel4=sc.vel)
+                   for (sc, k), t in zip(jobs, arr)]
             st = srv.run()
+            lat = []
+            for j in ids:
+                r = srv.job(j)
+                lat.append(r.finish_s - r.arrival_s)
             # plain path, FIFO through the same arrivals
-            fin, lat = 0.0, []
+            fin, plat = 0.0, []
             for t, sv in zip(arr, service):
                 fin = max(fin, t) + sv
-                lat.append(fin - t)
+                plat.append(fin - t)
+            parts = shard.gather({"updates": int(st.particle_updates), "wall": st.wall_s, "lat": lat,
+                                  "plain_wall": fin, "plain_lat": plat, "mean_active": st.mean_active,
+                                  "max_active": st.max_active, "substeps": int(st.substeps),
+                                  "launches": int(st.launches)})
+            served_updates = sum(p["updates"] for p in parts)
+            wall = max(p["wall"] for p in parts)
+            plain_wall = max(p["plain_wall"] for p in parts)
+            lat_all = [x for p in parts for x in p["lat"]]
+            plat_all = [x for p in parts for x in p["plain_lat"]]
             out["rates"][f"{rate:g}"] = {
-                "served": {"value": st.particle_updates / st.wall_s, "unit": UNIT,
-                           "p50_latency_s": st.p50_latency_s, "p99_latency_s": st.p99_latency_s,
-                           "wall_s": st.wall_s, "mean_active_scenes": st.mean_active,
+                "served": {"value": served_updates / wall, "unit": UNIT,
+                           "p50_latency_s": float(np.percentile(lat_all, 50)),
+                           "p99_latency_s": float(np.percentile(lat_all, 99)),
+                           "wall_s": wall, "mean_active_scenes": st.mean_active,
                            "max_active_scenes": st.max_active, "substeps": st.substeps,
-                           "gpu_launches": st.launches},
-                "plain_per_job": {"value": updates / fin, "unit": UNIT,
-                                  "p50_latency_s": float(np.percentile(lat, 50)),
-                                  "p99_latency_s": float(np.percentile(lat, 99)), "wall_s": fin},
-                "speedup": (st.particle_updates / st.wall_s) / (updates / fin)}
+                           "gpu_launches": sum(p["launches"] for p in parts)},
+                "plain_per_job": {"value": updates_all / plain_wall, "unit": UNIT,
+                                  "p50_latency_s": float(np.percentile(plat_all, 50)),
+                                  "p99_latency_s": float(np.percentile(plat_all, 99)), "wall_s": plain_wall},
+                "speedup": (served_updates / wall) / (updates_all / plain_wall)}
         out["capacity"] = {"particles": st.particle_capacity, "cells": st.cell_capacity}
     finally:
         srv.close()

@@ -51,3 +51,62 @@ def gather(obj, group=None):
     out = [None] * dist.get_world_size(group)
     dist.all_gather_object(out, obj, group=group)
     return out
+
+
+def scene_cost(scene, substeps):
+    """Particle-updates of `substeps` substeps of a scene: what a rank's share
+    costs on the device (the substep is bound per particle)."""
+    return int(scene.n) * int(substeps)
+
+
+class ShardedBatch:
+    """This rank's share of a list of independent scenes, advanced as one
+    batch on this rank's GPU (the multi-GPU form of the batched workload).
+
+    Scenes are assigned by `assign` on their particle-updates, so every rank
+    computes the same assignment without communicating; `gather_results`
+    brings every rank's per-scene results to every rank, keyed by the scene's
+    index in the full list.  `make_batch(particle_capacity, cell_capacity,
+    scene_capacity)` builds the batch (mls_mpm_b200.batch.Batch on the
+    device; any object with add_scene/step/sync/read works)."""
+
+    def __init__(self, scene_list, substeps, world_size, rank, make_batch=None, params=None):
+        if make_batch is None:
+            from .batch import Batch
+
+            def make_batch(p, c, s):
+                return Batch(p, c, s)
+        self.scenes = scene_list
+        self.rank = rank
+        self.mine = my_items([scene_cost(s, substeps) for s in scene_list], world_size, rank)
+        local = [scene_list[i] for i in self.mine]
+        self.particles = sum(s.n for s in local)
+        self.cells = sum(s.cells for s in local)
+        self.batch = make_batch(max(1, self.particles), max(1, self.cells), max(1, len(local)))
+        self.ids = {}
+        for i in self.mine:
+            p = params(scene_list[i]) if params is not None else None
+            self.ids[i] = self.batch.add_scene(scene_list[i], params=p)
+
+    def step(self, substeps):
+        self.batch.step(substeps)
+
+    def sync(self):
+        self.batch.sync()
+
+    def local_results(self, fn):
+        """{scene index: fn(batch, scene id)} for this rank's scenes."""
+        return {i: fn(self.batch, sid) for i, sid in self.ids.items()}
+
+    def gather_results(self, fn, group=None):
+        """Every rank's local_results(fn) merged, on every rank."""
+        merged = {}
+        for part in gather(self.local_results(fn), group):
+            merged.update(part)
+        return merged
+
+
+def shard_jobs(jobs, world_size, rank):
+    """Indices of the served jobs [(scene, substeps), ...] this rank runs
+    (assigned on particle-updates; arrival order is kept within a rank)."""
+    return my_items([scene_cost(sc, k) for sc, k in jobs], world_size, rank)

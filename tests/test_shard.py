@@ -87,3 +87,66 @@ def test_two_rank_gloo_sharded_run_matches_single_process():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert merged == _digests(range(len(_scene_list())))
+
+
+class _FakeBatch:
+    """Stands in for the device batch in the host-path test: records what the
+    rank built and returns a per-scene result computed on the host."""
+
+    def __init__(self, particles, cells, scenes):
+        self.capacity = (particles, cells, scenes)
+        self.added = []
+        self.steps = 0
+
+    def add_scene(self, scene, params=None):
+        self.added.append(scene)
+        return len(self.added) - 1
+
+    def step(self, k):
+        self.steps += k
+
+    def sync(self):
+        pass
+
+    def read(self, sid, name):
+        sc = self.added[sid]
+        return float(np.float64(sc.pos[:, :3]).sum()) + self.steps
+
+
+def _sharded_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sc = _scene_list()
+        sb = shard.ShardedBatch(sc, 7, world, rank, make_batch=_FakeBatch)
+        b = sb.batch
+        # this rank's batch holds exactly its share, sized to it
+        assert b.capacity == (sum(sc[i].n for i in sb.mine), sum(sc[i].cells for i in sb.mine), len(sb.mine))
+        sb.step(7)
+        sb.sync()
+        got = sb.gather_results(lambda batch, sid: batch.read(sid, "pos"))
+        jobs = [(s, 10 + i) for i, s in enumerate(sc)]
+        q.put((rank, sorted(sb.mine), got, shard.shard_jobs(jobs, world, rank)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_sharded_batch_host_path():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sharded_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=240) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    sc = _scene_list()
+    (r0, mine0, got0, jobs0), (r1, mine1, got1, jobs1) = res
+    # the two shares partition the scenes, and both ranks gathered every result
+    assert sorted(mine0 + mine1) == list(range(len(sc))) and not set(mine0) & set(mine1)
+    want = {i: float(np.float64(s.pos[:, :3]).sum()) + 7 for i, s in enumerate(sc)}
+    assert got0 == want and got1 == want
+    assert sorted(jobs0 + jobs1) == list(range(len(sc))) and not set(jobs0) & set(jobs1)
