@@ -200,13 +200,18 @@ def main():
     from mls_mpm_b200.abi import check
     scene = scenes.WORKLOADS[args.workload](seed=rank)
 
-    def make():
-        """One simulation of the workload; three identical copies follow the
-        same trajectory, so the device-timed, per-phase and end-to-end
-        numbers all cover the same substeps [W, W+K)."""
+    def make(render=False):
+        """One simulation of the workload; identical copies follow the same
+        trajectory, so the device-timed, per-phase and end-to-end numbers all
+        cover the same substeps [W, W+K).  render: the renderer takes its
+        buffers at start-up (as fluid-renderer.js binds them once), before
+        the warm-up."""
         fl = FluidGPU.from_scene(scene, device=local)
         if scene.diffuse_max:
             DiffuseGPU(scene.diffuse_max).initGPU(local, fl)
+        if render:
+            for name in ("pos", "vel", "density"):
+                fl.get_buffer(name)
         for _ in range(args.warmup):
             fl.simFrame()
         fl.sync()
@@ -260,7 +265,7 @@ def main():
     # without waiting; the clock stops after the last readback has landed.
     # The same loop without the render buffers is reported beside it.
     def e2e_run(render):
-        fl = make()
+        fl = make(render)
         X, Y, Z = scene.grid
         barrier()
         t0 = time.perf_counter()

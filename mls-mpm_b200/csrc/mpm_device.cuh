@@ -28,12 +28,12 @@ __device__ __forceinline__ int32_t encode(float v) {
     float c = fminf(fmaxf(v, -kEncodeClamp), kEncodeClamp);
     return __float2int_rz(c * kFixed);
 }
-// shaders.js:25 (IEEE division)
 // 1 when an encoded value sits at encode's clamp (|value| >= 20000 before
 // scaling): the health flag MPM_HEALTH_SATURATED.
 constexpr int32_t kEncodedMax = 2000000000;   // kEncodeClamp * kFixed, exact in f32
 __device__ __forceinline__ uint32_t at_clamp(int32_t e) { return (e == kEncodedMax || e == -kEncodedMax) ? 1u : 0u; }
 
+// shaders.js:25 (IEEE division)
 __device__ __forceinline__ float decode(int32_t v) { return __fdiv_rn(__int2float_rn(v), kFixed); }
 
 __device__ __forceinline__ float wclamp(float e, float lo, float hi) { return fminf(fmaxf(e, lo), hi); }

@@ -535,6 +535,49 @@ __device__ __forceinline__ PW particle_weights(float px, float py, float pz) {
 // encode() without the clamp, for values already known to lie in +-20000.
 __device__ __forceinline__ int32_t encode_unclamped(float v) { return __float2int_rz(v * kFixed); }
 
+// ---------------------------------------------------------------------------
+// Paired f32 arithmetic (add/mul.rn.f32x2): two independent lanes per
+// instruction, each lane rounded exactly as the scalar operation.  One rule
+// keeps every result bit-identical to the scalar sequence: a paired add never
+// takes a paired product directly as an operand (ptxas contracts that pair
+// into a fused multiply-add, which rounds once; measured on sm_100a, where a
+// paired product feeding scalar adds, or scalar products feeding a paired
+// add, stay separately rounded).  pmul: paired product; smul: two scalar
+// products as a pair; padd: paired add (operands never from pmul); sadd: two
+// scalar adds (for a pmul operand).  MPM_G2P_PACKED / MPM_MOM_PACKED turn
+// the paired forms on per kernel.
+// ---------------------------------------------------------------------------
+#ifndef MPM_G2P_PACKED
+#define MPM_G2P_PACKED 0
+#endif
+#ifndef MPM_MOM_PACKED
+#define MPM_MOM_PACKED 0
+#endif
+#if MPM_G2P_PACKED || MPM_MOM_PACKED
+__device__ __forceinline__ unsigned long long pk2(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 up2(unsigned long long r) {
+    float2 o;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+    return o;
+}
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a.x, a.y)), "l"(pk2(b.x, b.y)));
+    return up2(r);
+}
+__device__ __forceinline__ float2 smul(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a.x, a.y)), "l"(pk2(b.x, b.y)));
+    return up2(r);
+}
+__device__ __forceinline__ float2 sadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+#endif
+
 
 // ---------------------------------------------------------------------------
 // Chunks: the halo box of a chunk's cells in shared memory
@@ -1042,6 +1085,101 @@ __device__ __forceinline__ void mom_contrib_shared(const PW& w, const MomIn& in,
     mom_column<kClamp, 2, 2>(w, in, t, a0, a1, a2);
 }
 
+#if MPM_MOM_PACKED
+// mom_contrib_shared with the x and y components paired (paired f32 lanes):
+// each of the 81 values is the reference's own expression, as in mom_cell.
+struct MomTerms2 {
+    float dxs[3], dys[3];
+    float2 qz2[3], fz2[3];   // (x, y) lanes of C[.][2] dz_k and S[.][2] dz_k (scalar products)
+    float qzz[3], fzz[3];    // z lane
+    float2 axy0, axy1;       // (a00, a10), (a01, a11)
+    float2 sxy0, sxy1;       // (s00, s01), (s01, s11)
+    float a20, a21, s02, s12, coef;
+    float2 vxy, mm, cc;      // (vx, vy), (m, m), (coef, coef)
+};
+
+template <bool kClamp, int K, int J, int I>
+__device__ __forceinline__ void mom_cell2(const PW& w, const MomIn& in, const MomTerms2& t, float2 qxy, float qzz,
+                                          float2 gxy, float gz, int32_t* a0, int32_t* a1, int32_t* a2) {
+    const float ww = w.wx[I] * (w.wy[J] * w.wz[K]);
+    // x and y: w * (m * (v + Q) + coef * (G + S dz))
+    const float2 vq = padd(t.vxy, padd(qxy, t.qz2[K]));
+    const float2 tm = pmul(t.mm, vq);
+    const float2 f = pmul(t.cc, padd(gxy, t.fz2[K]));
+    const float2 r = pmul(make_float2(ww, ww), sadd(tm, f));
+    int32_t ex, ey;
+    if (kClamp) {
+        ex = encode(r.x);
+        ey = encode(r.y);
+    } else {
+        const float2 e = pmul(r, make_float2(kFixed, kFixed));
+        ex = __float2int_rz(e.x);
+        ey = __float2int_rz(e.y);
+    }
+    // z as mom_cell
+    const float Qz = qzz + t.qzz[K];
+    const float fzf = t.coef * (gz + t.fzz[K]);
+    const float vz = ww * (in.m * (in.vz + Qz) + fzf);
+    constexpr int o = K * kHXY + J * kHX + I;
+    atomicAdd(a0 + o, ex);
+    atomicAdd(a1 + o, ey);
+    atomicAdd(a2 + o, kClamp ? encode(vz) : encode_unclamped(vz));
+}
+
+template <bool kClamp, int J, int I>
+__device__ __forceinline__ void mom_column2(const PW& w, const MomIn& in, const MomTerms2& t, int32_t* a0,
+                                            int32_t* a1, int32_t* a2) {
+    const float dxi = t.dxs[I], dyj = t.dys[J];
+    const float2 dx2 = make_float2(dxi, dxi), dy2 = make_float2(dyj, dyj);
+    // (a00 dxi + a01 dyj, a10 dxi + a11 dyj) and (s00 dxi + s01 dyj, s01 dxi + s11 dyj)
+    const float2 qxy = padd(smul(t.axy0, dx2), smul(t.axy1, dy2));
+    const float qzz = t.a20 * dxi + t.a21 * dyj;
+    const float2 gxy = padd(smul(t.sxy0, dx2), smul(t.sxy1, dy2));
+    const float gz = t.s02 * dxi + t.s12 * dyj;
+    mom_cell2<kClamp, 0, J, I>(w, in, t, qxy, qzz, gxy, gz, a0, a1, a2);
+    mom_cell2<kClamp, 1, J, I>(w, in, t, qxy, qzz, gxy, gz, a0, a1, a2);
+    mom_cell2<kClamp, 2, J, I>(w, in, t, qxy, qzz, gxy, gz, a0, a1, a2);
+}
+
+template <bool kClamp>
+__device__ __forceinline__ void mom_contrib_shared2(const PW& w, const MomIn& in, const float* s, float coef,
+                                                    int32_t (*acc)[kHaloCells], int hb) {
+    MomTerms2 t;
+    const float s00 = s[0], s11 = s[1], s22 = s[2], s01 = s[3], s02 = s[4], s12 = s[5];
+    t.dxs[0] = -w.fx - 1.0f; t.dxs[1] = -w.fx; t.dxs[2] = 1.0f - w.fx;
+    t.dys[0] = -w.fy - 1.0f; t.dys[1] = -w.fy; t.dys[2] = 1.0f - w.fy;
+    const float dzs[3] = {-w.fz - 1.0f, -w.fz, 1.0f - w.fz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float2 dz2 = make_float2(dzs[k], dzs[k]);
+        t.qz2[k] = smul(make_float2(in.a02, in.a12), dz2);   // scalar: each feeds paired adds
+        t.qzz[k] = in.a22 * dzs[k];
+        t.fz2[k] = smul(make_float2(s02, s12), dz2);
+        t.fzz[k] = s22 * dzs[k];
+    }
+    t.axy0 = make_float2(in.a00, in.a10);
+    t.axy1 = make_float2(in.a01, in.a11);
+    t.sxy0 = make_float2(s00, s01);
+    t.sxy1 = make_float2(s01, s11);
+    t.a20 = in.a20; t.a21 = in.a21; t.s02 = s02; t.s12 = s12; t.coef = coef;
+    t.vxy = make_float2(in.vx, in.vy);
+    t.mm = make_float2(in.m, in.m);
+    t.cc = make_float2(coef, coef);
+    int32_t* a0 = &acc[0][hb];
+    int32_t* a1 = &acc[1][hb];
+    int32_t* a2 = &acc[2][hb];
+    mom_column2<kClamp, 0, 0>(w, in, t, a0, a1, a2);
+    mom_column2<kClamp, 0, 1>(w, in, t, a0, a1, a2);
+    mom_column2<kClamp, 0, 2>(w, in, t, a0, a1, a2);
+    mom_column2<kClamp, 1, 0>(w, in, t, a0, a1, a2);
+    mom_column2<kClamp, 1, 1>(w, in, t, a0, a1, a2);
+    mom_column2<kClamp, 1, 2>(w, in, t, a0, a1, a2);
+    mom_column2<kClamp, 2, 0>(w, in, t, a0, a1, a2);
+    mom_column2<kClamp, 2, 1>(w, in, t, a0, a1, a2);
+    mom_column2<kClamp, 2, 2>(w, in, t, a0, a1, a2);
+}
+#endif
+
 // Density of one particle from the staged halo masses (shaders.js:305-313):
 // the reference's k, j, i summation order, written out through template
 // indices.
@@ -1124,8 +1262,13 @@ __device__ __forceinline__ void mom_particle(const WorldView& v, const ChunkHdr&
     // health: the bound says encode's clamp may engage (a contribution may reach 20000)
     if (live && !safe) atomicOr(health, MPM_HEALTH_SATURATED);
     if (live && fast) {
+#if MPM_MOM_PACKED
+        if (safe) mom_contrib_shared2<false>(w, in, s, coef, acc, hb);
+        else mom_contrib_shared2<true>(w, in, s, coef, acc, hb);
+#else
         if (safe) mom_contrib_shared<false>(w, in, s, coef, acc, hb);
         else mom_contrib_shared<true>(w, in, s, coef, acc, hb);
+#endif
     } else if (live) {
         auto sink = [&](int k, int j, int i, int32_t ex, int32_t ey, int32_t ez) {
             const uint32_t cidx = baseIdx + (uint32_t)k * SLICE + (uint32_t)j * X + (uint32_t)i;
@@ -1550,6 +1693,48 @@ __device__ __noinline__ void g2p_direct_particle(const G2POut o, const SceneDesc
     o.rank[p] = g2p_store(o, sd, p, q, vi, o.dens[p], r.gv[0], r.gv[1], r.gv[2], r.B, ro, mirror);
 }
 
+#if MPM_G2P_PACKED
+// The 27-cell gather of G2P (shaders.js:606-629) with the x and y lanes of
+// each accumulation paired: (gvx, gvy), (B00, B10), (B01, B11), (B02, B12),
+// (B20, B21); every element keeps the reference's products and summation
+// order.  vb: the staged halo at the stencil base.
+__device__ __forceinline__ void g2p_gather_packed(const PW& w, const float4 q, const float4* vb, float& gvx,
+                                                  float& gvy, float& gvz, float* B) {
+    const int32_t bx = w.cx - 1, by = w.cy - 1, bz = w.cz - 1;
+    float2 gxy = make_float2(0.0f, 0.0f), b0 = gxy, b1 = gxy, b2 = gxy, b3 = gxy;
+    float gz = 0.0f, b22 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float wzk = w.wz[k];
+        const float dzk = __int2float_rn(bz + k) - q.z + 0.5f;
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+            const float wyzk = w.wy[jj] * wzk;
+            const float dyj = __int2float_rn(by + jj) - q.y + 0.5f;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float ww = w.wx[i] * wyzk;
+                const float dxi = __int2float_rn(bx + i) - q.x + 0.5f;
+                const float4 c = vb[k * kHXY + jj * kHX + i];
+                const float2 wvxy = pmul(make_float2(ww, ww), make_float2(c.x, c.y));
+                const float wvz = ww * c.z;
+                gxy = sadd(gxy, wvxy);
+                gz += wvz;
+                b0 = sadd(b0, pmul(wvxy, make_float2(dxi, dxi)));
+                b1 = sadd(b1, pmul(wvxy, make_float2(dyj, dyj)));
+                b2 = sadd(b2, pmul(wvxy, make_float2(dzk, dzk)));
+                b3 = padd(b3, smul(make_float2(wvz, wvz), make_float2(dxi, dyj)));
+                b22 += wvz * dzk;
+            }
+        }
+    }
+    gvx = gxy.x; gvy = gxy.y; gvz = gz;
+    B[0] = b0.x; B[1] = b1.x; B[2] = b2.x;
+    B[3] = b0.y; B[4] = b1.y; B[5] = b2.y;
+    B[6] = b3.x; B[7] = b3.y; B[8] = b22;
+}
+#endif
+
 template <uint32_t kC>
 __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(WorldView v, const float4* __restrict__ posm,
                                                               const float4* __restrict__ velid,
@@ -1639,6 +1824,9 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
             }
             float gvx = 0.0f, gvy = 0.0f, gvz = 0.0f;
             float B[9] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#if MPM_G2P_PACKED
+            g2p_gather_packed(w, q, vh + halo_base(h, w.cx, w.cy, w.cz), gvx, gvy, gvz, B);
+#else
             {
                 const int32_t bx = w.cx - 1, by = w.cy - 1, bz = w.cz - 1;
                 const int hb = halo_base(h, w.cx, w.cy, w.cz);
@@ -1664,6 +1852,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
                     }
                 }
             }
+#endif
             const uint32_t rk = g2p_store(out, sd, p, q, vi, dns[r], gvx, gvy, gvz, B, ro, mirror);
             // the previous particle's rank: its atomic has long returned
             if (pend_p != kHole) v.rank[pend_p] = pend_rank;
