@@ -180,12 +180,19 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-one-at-a-time comparison")
     ap.add_argument("--no-served", action="store_true", help="skip the served-vs-per-job comparison")
     ap.add_argument("--no-drift", action="store_true", help="skip the f32-vs-f64 drift report")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched-vs-one-at-a-time comparison and print it (for profiling)")
     ap.add_argument("--workload", default=WORKLOAD)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference_arm(args, ws, rank)
+    if args.batched_only:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"batched": batched_comparison(local, substeps=args.steps, warmup=args.warmup)}))
+        return 0
 
     import torch
     torch.cuda.set_device(local)

@@ -114,7 +114,7 @@ static void free_scene(Scene& s) {
                     s.diffuse.kill_bits, s.diffuse.alive_mask, s.diffuse.block_counts, s.diffuse.kill_counts,
                     s.diffuse.rank_state,
                     s.diffuse.staging,
-                    s.diffuse.top_hist,
+                    s.diffuse.top_hist, s.diffuse.tail_P, s.diffuse.tail_W,
                     s.edit_pos, s.edit_vel, s.edit_mass, s.edit_blocks, s.edit_word, s.diffuse.gen_dev,
                     s.diffuse.adv_dev};
     for (void* p : ptrs) dfree(p);
@@ -124,6 +124,9 @@ static void free_scene(Scene& s) {
         if (ev) cudaEventDestroy(ev);
     if (s.diffuse.rb_after) cudaEventDestroy(s.diffuse.rb_after);
     if (s.diffuse.rb_stream) cudaStreamDestroy(s.diffuse.rb_stream);
+    if (s.diffuse.fork_ev) cudaEventDestroy(s.diffuse.fork_ev);
+    if (s.diffuse.join_ev) cudaEventDestroy(s.diffuse.join_ev);
+    if (s.diffuse.side) cudaStreamDestroy(s.diffuse.side);
     if (s.edit_host) cudaFreeHost(s.edit_host);
     if (s.stream) cudaStreamDestroy(s.stream);
 }
@@ -216,13 +219,51 @@ static cudaError_t guard_top_history(Scene& s) {
     constexpr uint32_t R = DiffuseState::kAliveRing;
     for (uint32_t i = d.alive_tail; i != d.alive_head; ++i) {
         const uint32_t t = i % R;
-        if (d.alive_pass[t] != UINT64_MAX && d.alive_pass[t] + DiffuseState::kTopHist <= d.passes) {
+        if (d.alive_issued[t] && d.alive_pass[t] != UINT64_MAX &&
+            d.alive_pass[t] + DiffuseState::kTopHist <= d.passes) {
             const cudaError_t e = cudaStreamWaitEvent(s.stream, d.alive_ev[t], 0);
             if (e != cudaSuccess) return e;
             d.alive_pass[t] = UINT64_MAX;
         }
     }
     return cudaSuccess;
+}
+
+// Binned engine: the alive readbacks requested while the kill pass they read
+// was deferred, once that pass has been enqueued: copy its top_hist entry on
+// the readback stream after the point the scene stream has reached.
+static cudaError_t issue_readbacks(Scene& s) {
+    DiffuseState& d = s.diffuse;
+    if (!d.enabled) return cudaSuccess;
+    constexpr uint32_t R = DiffuseState::kAliveRing;
+    bool ordered = false;
+    for (uint32_t i = d.alive_tail; i != d.alive_head; ++i) {
+        const uint32_t h = i % R;
+        if (d.alive_issued[h] || d.alive_pass[h] >= d.passes) continue;
+        cudaError_t e = cudaSuccess;
+        if (!ordered) {
+            e = cudaEventRecord(d.rb_after, s.stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(d.rb_stream, d.rb_after, 0);
+            ordered = true;
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d.alive_ring + h, d.top_hist + d.alive_pass[h] % DiffuseState::kTopHist, 4,
+                                cudaMemcpyDeviceToHost, d.rb_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(d.alive_ev[h], d.rb_stream);
+        if (e != cudaSuccess) return e;
+        d.alive_issued[h] = true;
+    }
+    return cudaSuccess;
+}
+
+// Binned engine: run a deferred diffuse tail now (every call that observes or
+// changes the scene does, so it sees the state the reference would after the
+// last step).
+static cudaError_t flush_tail(Scene& s) {
+    if (s.engine != kEngineBinned || !s.diffuse.tail_pending) return cudaSuccess;
+    cudaError_t e = world_flush_diffuse(s);
+    if (e == cudaSuccess) e = issue_readbacks(s);
+    return e;
 }
 
 static cudaError_t launch_substep(Scene& s) {
@@ -414,6 +455,7 @@ mpm_status mpm_upload_particles(mpm_scene* sc, const float* pos4, const float* v
     if (n > s.capacity) return fail(MPM_ERR_CAPACITY, "n exceeds particle capacity");
     if (const mpm_status bad = plain_positions_ok(s, pos4, n)) return bad;
     DeviceGuard guard(s.device);
+    CUDA_TRY(flush_tail(s), "diffuse");
     cudaStream_t st = s.stream;
     CUDA_TRY(cudaMemcpyAsync(s.pos, pos4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "upload pos");
     if (vel4) CUDA_TRY(cudaMemcpyAsync(s.vel, vel4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "upload vel");
@@ -440,6 +482,7 @@ mpm_status mpm_set_params(mpm_scene* sc, const mpm_params* p) {
     if (s.engine == kEngineBinned && s.world_slot >= 0 && p->particle_num != s.world.scenes[s.world_slot].n) {
         // active count changed (spawn / delete): reload the working state next step
         DeviceGuard guard(s.device);
+        CUDA_TRY(flush_tail(s), "diffuse");
         CUDA_TRY(sync_reference_buffers(s), "export");
         s.fast_stale = true;
     }
@@ -486,6 +529,11 @@ mpm_status mpm_diffuse_enable(mpm_scene* sc, uint32_t max_count, const mpm_gen_p
     if (e == cudaSuccess) e = dalloc(&d.top_hist, DiffuseState::kTopHist * 4);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d.rb_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d.rb_after, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d.side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d.fork_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d.join_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = dalloc(&d.tail_P, sizeof(mpm_params));
+    if (e == cudaSuccess) e = dalloc(&d.tail_W, sizeof(mpm_wall_params));
     if (e == cudaSuccess) e = dalloc(&d.staging, N * 48);
     if (e == cudaSuccess) e = dalloc(&d.gen_dev, sizeof(mpm_gen_params));
     if (e == cudaSuccess) e = dalloc(&d.adv_dev, sizeof(mpm_advect_params));
@@ -537,6 +585,7 @@ mpm_status mpm_step(mpm_scene* sc, int substeps) {
     Scene& s = sc->s;
     DeviceGuard guard(s.device);
     if (s.engine == kEngineBinned && s.fast_stale) {
+        CUDA_TRY(flush_tail(s), "diffuse");
         cudaError_t e = import_state(s);
         if (e != cudaSuccess) return cuda_fail(e, "import");
     }
@@ -544,6 +593,7 @@ mpm_status mpm_step(mpm_scene* sc, int substeps) {
         cudaError_t e = launch_substep(s);
         if (e != cudaSuccess) return cuda_fail(e, "mpm_step launch");
     }
+    if (s.engine == kEngineBinned) CUDA_TRY(issue_readbacks(s), "alive readbacks");
     return MPM_OK;
 }
 
@@ -561,6 +611,7 @@ static mpm_status health_status(Scene& s) {
 mpm_status mpm_sync(mpm_scene* sc) {
     if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     DeviceGuard guard(sc->s.device);
+    CUDA_TRY(flush_tail(sc->s), "diffuse");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "mpm_sync");
     // queued alive-count readbacks have landed too
     if (sc->s.diffuse.rb_stream) CUDA_TRY(cudaStreamSynchronize(sc->s.diffuse.rb_stream), "mpm_sync readbacks");
@@ -570,6 +621,7 @@ mpm_status mpm_sync(mpm_scene* sc) {
 mpm_status mpm_wait(mpm_scene* sc, double timeout_s) {
     if (!sc || !(timeout_s >= 0.0)) return fail(MPM_ERR_INVALID_ARG, "NULL scene or negative timeout");
     DeviceGuard guard(sc->s.device);
+    CUDA_TRY(flush_tail(sc->s), "diffuse");
     const auto t0 = std::chrono::steady_clock::now();
     for (;;) {
         cudaError_t e = cudaStreamQuery(sc->s.stream);
@@ -596,6 +648,10 @@ mpm_status mpm_get_buffer(mpm_scene* sc, mpm_buffer which, void** dev_ptr, size_
     if (!sc || !dev_ptr || !bytes) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     if (!buffer_info(sc->s, which, dev_ptr, bytes)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_exported = true;
+    {
+        DeviceGuard guard(sc->s.device);
+        CUDA_TRY(flush_tail(sc->s), "diffuse");
+    }
     if (is_particle_buffer(which)) {
         Scene& s = sc->s;
         DeviceGuard guard(s.device);
@@ -633,6 +689,7 @@ mpm_status mpm_get_ipc_handle(mpm_scene* sc, mpm_buffer which, void* handle, siz
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_exported = true;
     DeviceGuard guard(sc->s.device);
+    CUDA_TRY(flush_tail(sc->s), "diffuse");
     if (is_particle_buffer(which)) {
         Scene& s = sc->s;
         CUDA_TRY(ensure_reference(s, which), "export");
@@ -660,6 +717,7 @@ mpm_status mpm_download(mpm_scene* sc, mpm_buffer which, void* host_dst, size_t 
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
     DeviceGuard guard(sc->s.device);
+    CUDA_TRY(flush_tail(sc->s), "diffuse");
     CUDA_TRY(ensure_reference(sc->s, which), "export");
     CUDA_TRY(cudaMemcpyAsync(host_dst, p, bytes, cudaMemcpyDeviceToHost, sc->s.stream), "download");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "download sync");
@@ -671,7 +729,6 @@ mpm_status mpm_upload(mpm_scene* sc, mpm_buffer which, const void* host_src, siz
     void* p;
     size_t sz;
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
-    if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_written = true;
     if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
     if (which == MPM_BUF_POS && sc->s.engine == kEnginePlain) {
         if (bytes % 16) return fail(MPM_ERR_INVALID_ARG, "plain engine: positions are uploaded as whole vec4 records");
@@ -679,6 +736,8 @@ mpm_status mpm_upload(mpm_scene* sc, mpm_buffer which, const void* host_src, siz
             return bad;
     }
     DeviceGuard guard(sc->s.device);
+    CUDA_TRY(flush_tail(sc->s), "diffuse");   // before the upload replaces what the tail would write
+    if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_written = true;
     if (is_particle_buffer(which)) {
         CUDA_TRY(sync_reference_buffers(sc->s), "export");
         if (sc->s.engine == kEngineBinned) sc->s.fast_stale = true;
@@ -695,6 +754,7 @@ mpm_status mpm_diffuse_alive_count(mpm_scene* sc, int32_t* alive) {
     DiffuseState& d = sc->s.diffuse;
     if (!d.enabled) return fail(MPM_ERR_INVALID_ARG, "diffuse not enabled");
     DeviceGuard guard(sc->s.device);
+    CUDA_TRY(flush_tail(sc->s), "diffuse");
     CUDA_TRY(cudaMemcpyAsync(d.host_top, d.top, 4, cudaMemcpyDeviceToHost, sc->s.stream), "top readback");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "top sync");
     *alive = (int32_t)d.max_count - *d.host_top;
@@ -703,33 +763,45 @@ mpm_status mpm_diffuse_alive_count(mpm_scene* sc, int32_t* alive) {
 
 mpm_status mpm_diffuse_request_alive(mpm_scene* sc) {
     if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
-    DiffuseState& d = sc->s.diffuse;
+    Scene& s = sc->s;
+    DiffuseState& d = s.diffuse;
     if (!d.enabled) return fail(MPM_ERR_INVALID_ARG, "diffuse not enabled");
-    DeviceGuard guard(sc->s.device);
+    DeviceGuard guard(s.device);
     constexpr uint32_t R = DiffuseState::kAliveRing;
     if (d.alive_head - d.alive_tail == R) {   // every slot in flight: take the oldest
         const uint32_t t = d.alive_tail % R;
+        if (!d.alive_issued[t]) CUDA_TRY(flush_tail(s), "diffuse");   // its kill pass is still deferred
         CUDA_TRY(cudaEventSynchronize(d.alive_ev[t]), "alive readback wait");
         d.alive_last = (int32_t)d.max_count - d.alive_ring[t];
         ++d.alive_tail;
     }
     const uint32_t h = d.alive_head % R;
-    if (d.passes == 0 || d.top_written || d.top_exported) {
-        // top may differ from the last kill pass's: copy it in stream order
-        CUDA_TRY(cudaMemcpyAsync(d.alive_ring + h, d.top, 4, cudaMemcpyDeviceToHost, sc->s.stream), "alive readback");
-        CUDA_TRY(cudaEventRecord(d.alive_ev[h], sc->s.stream), "alive readback event");
+    if (d.top_written || d.top_exported || (d.passes == 0 && !d.tail_pending)) {
+        // top may differ from the last kill pass's: copy it in stream order,
+        // after the deferred tail
+        CUDA_TRY(flush_tail(s), "diffuse");
+        CUDA_TRY(cudaMemcpyAsync(d.alive_ring + h, d.top, 4, cudaMemcpyDeviceToHost, s.stream), "alive readback");
+        CUDA_TRY(cudaEventRecord(d.alive_ev[h], s.stream), "alive readback event");
         d.alive_pass[h] = UINT64_MAX;
+        d.alive_issued[h] = true;
+    } else if (d.tail_pending) {
+        // the top this readback reads is what the deferred kill pass (the
+        // passes-th) records in top_hist: the copy is issued once that pass is
+        // enqueued (the next step or a flush)
+        d.alive_pass[h] = d.passes;
+        d.alive_issued[h] = false;
     } else {
         // top is what the latest kill pass left in top_hist: copy that entry on
         // the side stream once the scene stream gets here, without holding the
         // scene stream back
         const uint64_t k = d.passes - 1;
-        CUDA_TRY(cudaEventRecord(d.rb_after, sc->s.stream), "alive readback point");
+        CUDA_TRY(cudaEventRecord(d.rb_after, s.stream), "alive readback point");
         CUDA_TRY(cudaStreamWaitEvent(d.rb_stream, d.rb_after, 0), "alive readback order");
         CUDA_TRY(cudaMemcpyAsync(d.alive_ring + h, d.top_hist + k % DiffuseState::kTopHist, 4, cudaMemcpyDeviceToHost,
                                  d.rb_stream), "alive readback");
         CUDA_TRY(cudaEventRecord(d.alive_ev[h], d.rb_stream), "alive readback event");
         d.alive_pass[h] = k;
+        d.alive_issued[h] = true;
     }
     ++d.alive_head;
     return MPM_OK;
@@ -744,6 +816,7 @@ mpm_status mpm_diffuse_poll_alive(mpm_scene* sc, int32_t* alive, int32_t* ready)
     int32_t got = 0;
     while (d.alive_tail != d.alive_head) {
         const uint32_t t = d.alive_tail % R;
+        if (!d.alive_issued[t]) break;   // its copy waits for a deferred kill pass
         const cudaError_t q = cudaEventQuery(d.alive_ev[t]);
         if (q == cudaErrorNotReady) break;
         if (q != cudaSuccess) return cuda_fail(q, "alive readback query");
@@ -795,6 +868,7 @@ mpm_status mpm_delete_near(mpm_scene* sc, const double origin[3], const double d
     Scene& s = sc->s;
     DeviceGuard guard(s.device);
     CUDA_TRY(ensure_edit_scratch(s, true), "deleteNear scratch");
+    CUDA_TRY(flush_tail(s), "diffuse");
     CUDA_TRY(sync_reference_buffers(s), "export");
     const mpm_ray_params del = pack_ray(origin, dir, radius);
     const uint32_t n = s.params.particle_num;
@@ -823,6 +897,7 @@ mpm_status mpm_raycast_fluid(mpm_scene* sc, const double origin[3], const double
     Scene& s = sc->s;
     DeviceGuard guard(s.device);
     CUDA_TRY(ensure_edit_scratch(s, false), "raycast scratch");
+    CUDA_TRY(flush_tail(s), "diffuse");
     CUDA_TRY(sync_reference_buffers(s), "export");
     const mpm_ray_params ray = pack_ray(origin, dir, radius);
     CUDA_TRY(launch_raycast(ray, s.params.particle_num, s.pos, s.edit_word, s.stream), "raycast");
@@ -853,6 +928,7 @@ mpm_status mpm_append_particles(mpm_scene* sc, const float* pos4, const float* v
     if (const mpm_status bad = plain_positions_ok(s, pos4, n)) return bad;
     DeviceGuard guard(s.device);
     cudaStream_t st = s.stream;
+    CUDA_TRY(flush_tail(s), "diffuse");
     CUDA_TRY(sync_reference_buffers(s), "export");
     CUDA_TRY(cudaMemcpyAsync(s.pos + start, pos4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "append pos");
     if (vel4) CUDA_TRY(cudaMemcpyAsync(s.vel + start, vel4, (size_t)n * 16, cudaMemcpyHostToDevice, st), "append vel");
@@ -899,6 +975,8 @@ const char* mpm_phase_name(int phase) {
 
 mpm_status mpm_profile_enable(mpm_scene* sc, int on) {
     if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
+    DeviceGuard guard(sc->s.device);
+    CUDA_TRY(flush_tail(sc->s), "diffuse");
     sc->s.profile = on != 0;
     return MPM_OK;
 }
@@ -907,6 +985,7 @@ mpm_status mpm_profile_read(mpm_scene* sc, double* ms, uint64_t* count, int rese
     if (!sc) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     Scene& s = sc->s;
     DeviceGuard guard(s.device);
+    CUDA_TRY(flush_tail(s), "diffuse");
     CUDA_TRY(s.drain_profile(), "mpm_profile_read");
     for (int i = 0; i < MPM_PHASE_COUNT; ++i) {
         if (ms) ms[i] = s.prof_ms[i];

@@ -819,9 +819,10 @@ cudaError_t launch_apply_hand(Scene& s) {
 // DiffuseGPU.step (diffuse-gpu.js:148-166) after G2P.  With eval the spawn
 // decision pass runs here (plain engine); the binned engine makes that
 // decision in its G2P epilogue and has already bumped the seed.
-cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const mpm_wall_params* W_dev) {
+cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev, const mpm_wall_params* W_dev,
+                           cudaStream_t stream) {
     static_assert(kThreads == (int)kGroupIds, "one rank group per 256-thread block");
-    cudaStream_t st = s.stream;
+    cudaStream_t st = stream ? stream : s.stream;
     const mpm_params& P = s.params;
     DiffuseState& d = s.diffuse;
     const uint32_t n = P.particle_num;

@@ -19,8 +19,9 @@ cudaError_t launch_alive_mask_build(Scene& s);
 // DiffuseGPU.step after G2P; eval = run the spawn-decision pass here.
 // P_dev / W_dev (binned engine): the scene's uniforms in device memory, read
 // by ADVECT instead of the host copies, so the launches can be captured in a
-// CUDA graph and replayed with uniforms uploaded later.
+// CUDA graph and replayed with uniforms uploaded later.  stream: where to
+// enqueue (null: the scene's stream).
 cudaError_t launch_diffuse(Scene& s, bool eval, const mpm_params* P_dev = nullptr,
-                           const mpm_wall_params* W_dev = nullptr);
+                           const mpm_wall_params* W_dev = nullptr, cudaStream_t stream = nullptr);
 
 }  // namespace mpm

@@ -58,6 +58,21 @@ struct DiffuseState {
     cudaEvent_t rb_after = nullptr;         // scene-stream point a readback copies after
     mpm_gen_params* gen_dev = nullptr;      // device GenParams (binned engine: seed bumped on the device)
     mpm_advect_params* adv_dev = nullptr;   // device copy of adv (binned engine)
+    // Binned engine: DiffuseGPU.step of the last substep (spawn pass, ADVECT,
+    // kill pass) is deferred and runs on a side stream beside the next
+    // substep's binning, P2G_MASS, DECODE_MASS and P2G_MOM, joining before its
+    // UPDATE_GRID (the first pass that writes what the tail reads).  Any call
+    // that observes or changes the scene runs a pending tail first (flush).
+    bool tail_pending = false;
+    cudaStream_t side = nullptr;            // the tail's stream
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // the uniforms of the substep the pending tail belongs to (copied on the
+    // device after its G2P, so later uploads of the scene table do not reach it)
+    mpm_params* tail_P = nullptr;
+    mpm_wall_params* tail_W = nullptr;
+    // readbacks requested while the kill pass they read was still deferred:
+    // issued once that pass is enqueued
+    bool alive_issued[kAliveRing] = {true, true, true, true};
 };
 
 // Engines: the binned item-major substep (default) and the plain per-pass

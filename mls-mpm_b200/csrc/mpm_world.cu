@@ -1995,7 +1995,7 @@ void world_free(World& w) {
         w.h_stage[b] = nullptr;
         w.stage_ev[b] = nullptr;
     }
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < World::kGraphs; ++b)
         if (w.graph[b]) cudaGraphExecDestroy(w.graph[b]);
     world_arrays(w, [](auto*& p, size_t) {
         dfree(p);
@@ -2210,7 +2210,10 @@ cudaError_t world_export_scene(World& w, int slot, float4* pos, float4* vel, flo
 // (its diffuse update runs when enabled, its profiler times the phases; null
 // in a graph capture without diffuse, and for batches); ro: the owner's
 // reference-layout mirrors.
-static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro) {
+// tail_in: ds's deferred diffuse tail of the previous substep runs on its side
+// stream beside this substep's first passes; defer: this substep's tail is
+// left pending (else it runs at the end, in stream order).
+static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro, bool tail_in, bool defer) {
     const WorldView v = w.view();
     cudaStream_t st = w.stream;
     const int cur = w.cur, nxt = cur ^ 1;
@@ -2233,6 +2236,18 @@ static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro) {
     }
     Scene* prof = ds;
     cudaError_t e;
+    if (tail_in) {
+        // DiffuseGPU.step of the previous substep (spawn pass, ADVECT, kill pass)
+        // reads the pool, the free list, vel4 and its own copy of the uniforms,
+        // none of which the binning, P2G_MASS, DECODE_MASS or P2G_MOM touch
+        DiffuseState& d = ds->diffuse;
+        e = cudaEventRecord(d.fork_ev, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(d.side, d.fork_ev, 0);
+        if (e == cudaSuccess) e = launch_diffuse(*ds, false, d.tail_P, d.tail_W, d.side);
+        if (e == cudaSuccess) e = cudaEventRecord(d.join_ev, d.side);
+        if (e != cudaSuccess) return e;
+        d.tail_pending = false;
+    }
     {
         Phase ph(prof, MPM_PHASE_SORT);
         if (!w.counted) {
@@ -2281,6 +2296,12 @@ static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro) {
                                                                             w.aff[cur], w.cmf, mv, w.dens);
         w.launches++;
     }
+    // the tail's ADVECT reads vel4 and its spawn pass the spawn bits that
+    // UPDATE_GRID and G2P are about to rewrite
+    if (tail_in) {
+        e = cudaStreamWaitEvent(st, ds->diffuse.join_ev, 0);
+        if (e != cudaSuccess) return e;
+    }
     {
         Phase ph(prof, MPM_PHASE_UPDATE_GRID);   // includes APPLY_HAND
         k_update_tiles<<<w.grid_blocks, 256, 0, st>>>(v, cm, mv, w.mvf, w.vel4, cm_n, mv_n);
@@ -2311,9 +2332,26 @@ static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro) {
     if (dv.enabled) {
         ds->diffuse.seed += 1u;   // mirrors the device-side bump in k_tile_scan_top
         const SceneDesc* sd_dev = w.d_scenes + dv.scene;
-        e = launch_diffuse(*ds, false, &sd_dev->P, &sd_dev->W);
+        if (defer) {
+            // this substep's uniforms for its deferred tail (the scene table may
+            // be rewritten before the tail runs)
+            DiffuseState& d = ds->diffuse;
+            e = cudaMemcpyAsync(d.tail_P, &sd_dev->P, sizeof(mpm_params), cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d.tail_W, &sd_dev->W, sizeof(mpm_wall_params), cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess) d.tail_pending = true;
+        } else {
+            e = launch_diffuse(*ds, false, &sd_dev->P, &sd_dev->W);
+        }
     }
     return e;
+}
+
+cudaError_t world_flush_diffuse(Scene& s) {
+    DiffuseState& d = s.diffuse;
+    if (!d.tail_pending) return cudaSuccess;
+    d.tail_pending = false;
+    return launch_diffuse(s, false, d.tail_P, d.tail_W, s.stream);
 }
 
 cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
@@ -2336,12 +2374,19 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
     if (e != cudaSuccess) return e;
     const bool diffuse = ds && ds->diffuse.enabled;
     const bool profiling = ds && ds->profile;
+    if (profiling && diffuse && ds->diffuse.tail_pending) {
+        // phases are timed on the scene stream: no tail beside them
+        e = world_flush_diffuse(*ds);
+        if (e != cudaSuccess) return e;
+    }
+    const bool tail_in = diffuse && ds->diffuse.tail_pending;
+    const bool defer = diffuse && !profiling;
     // a substep that must recount runs eagerly; the captured graphs never count
-    if (!use_graph || profiling || !w.counted) return enqueue_substep(w, ds, ro);
+    if (!use_graph || profiling || !w.counted) return enqueue_substep(w, ds, ro, tail_in, defer);
     // the diffuse update joins the graph: its kernels read the uniforms from
-    // the device scene table and the advect parameters from a device copy
+    // device copies and the advect parameters from a device copy
     Scene* dsc = diffuse ? ds : nullptr;
-    const int p = w.cur;   // cur and gbuf flip together: one graph per parity
+    const int p = 2 * w.cur + (tail_in ? 1 : 0);   // cur and gbuf flip together: graphs per parity
     const bool mirror = ro.enabled != 0;
     if (!w.graph[p] || w.graph_gen[p] != w.generation || w.graph_diffuse[p] != diffuse ||
         w.graph_mirror[p] != mirror) {
@@ -2356,10 +2401,12 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
         const uint64_t sl0 = dsc ? dsc->launches : 0;
         const uint32_t seed0 = dsc ? dsc->diffuse.seed : 0;
         const uint64_t passes0 = dsc ? dsc->diffuse.passes : 0;
+        const bool pending0 = dsc ? dsc->diffuse.tail_pending : false;
+        const bool written0 = dsc ? dsc->diffuse.top_written : false;
         cudaGraph_t g = nullptr;
         e = cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;
-        const cudaError_t e2 = enqueue_substep(w, dsc, ro);
+        const cudaError_t e2 = enqueue_substep(w, dsc, ro, tail_in, defer);
         e = cudaStreamEndCapture(w.stream, &g);
         if (e2 != cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaGraphInstantiate(&w.graph[p], g, 0);
@@ -2375,6 +2422,8 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
             dsc->launches = sl0;
             dsc->diffuse.seed = seed0;
             dsc->diffuse.passes = passes0;
+            dsc->diffuse.tail_pending = pending0;
+            dsc->diffuse.top_written = written0;
         }
         if (e != cudaSuccess) {
             w.graph[p] = nullptr;
@@ -2390,8 +2439,11 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
     w.launches += w.graph_kernels[p];
     if (dsc) {
         dsc->diffuse.seed += 1u;
-        dsc->diffuse.passes += 1u;   // the graph's kill pass
-        dsc->diffuse.top_written = false;
+        if (tail_in) {
+            dsc->diffuse.passes += 1u;   // the previous substep's kill pass ran in the graph
+            dsc->diffuse.top_written = false;
+        }
+        dsc->diffuse.tail_pending = true;   // this substep's tail waits for the next one
     }
     w.pos_bound = w.n_total;   // the layout after a substep is dense
     w.cm_current = w.grid_i32[w.gbuf];

@@ -214,12 +214,15 @@ struct World {
     float4* vel4 = nullptr;                      // cells: (vx, vy, vz, 0), the same velocities 16-byte aligned
     uint32_t* health = nullptr;                  // scene_cap words: MPM_HEALTH_* bits per scene slot
 
-    // CUDA graphs of one substep (one per buffer parity), valid for `generation`
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    uint64_t graph_gen[2] = {0, 0};
-    uint64_t graph_kernels[2] = {0, 0};     // kernels in each graph (launch accounting)
-    bool graph_diffuse[2] = {false, false};  // the graph includes the diffuse update of its scene
-    bool graph_mirror[2] = {false, false};   // the graph writes the owner's reference-layout mirrors
+    // CUDA graphs of one substep, one per buffer parity and per whether a
+    // deferred diffuse tail runs inside it (index 2 * parity + tail), valid
+    // for `generation`
+    static constexpr int kGraphs = 4;
+    cudaGraphExec_t graph[kGraphs] = {};
+    uint64_t graph_gen[kGraphs] = {};
+    uint64_t graph_kernels[kGraphs] = {};    // kernels in each graph (launch accounting)
+    bool graph_diffuse[kGraphs] = {};        // the graph includes the diffuse update of its scene
+    bool graph_mirror[kGraphs] = {};         // the graph writes the owner's reference-layout mirrors
 
     WorldView view() const;
 };
@@ -256,5 +259,8 @@ struct Scene;
 // null for batches).  use_graph: replay a captured CUDA graph of the substep
 // (captured on first use and whenever the scene set changes).
 cudaError_t world_substep(World& w, Scene* owner, bool use_graph);
+// Runs the owner's deferred diffuse tail now, in stream order (no-op when
+// none is pending).
+cudaError_t world_flush_diffuse(Scene& owner);
 
 }  // namespace mpm

@@ -84,3 +84,38 @@ def test_readback_value_as_of_request(gpu, engine):
         assert _poll(lib, g) == (after, 1)
     finally:
         g.close()
+
+
+def test_readback_requested_right_after_steps(gpu):
+    """Binned engine: a step leaves its DiffuseGPU.step (spawn, ADVECT, kill)
+    to run beside the next step's first passes; a readback requested right
+    after the step still reports the count that step leaves.  The same frames
+    on a second scene, read synchronously after every step, give the values."""
+    sc = scenarios.walls_hand_diffuse()
+    frames = list(sc.frames())
+    lib = gpu
+    ref = GpuScene(lib, sc.scene, sc.diffuse_max)
+    g = GpuScene(lib, sc.scene, sc.diffuse_max)
+    try:
+        want = []
+        for i in range(len(frames)):
+            ref.frame(*frames[i][:4])
+            want.append(_alive_sync(lib, ref))
+        assert len(set(want)) > 3          # the count moves
+        last = -1
+        for i in range(len(frames)):
+            g.frame(*frames[i][:4])
+            _request(lib, g)
+            a, ready = _poll(lib, g)        # never waits; what landed is some earlier step's count
+            if ready:
+                k = want.index(a, last + 1 if last + 1 < len(want) else 0)
+                assert k <= i
+                last = k
+        check(lib.mpm_sync(g.h), "mpm_sync")
+        assert _poll(lib, g) == (want[-1], 1)
+        # the whole state equals the reference scene's
+        from runner import diff_report
+        assert not diff_report(g.state(), ref.state())
+    finally:
+        g.close()
+        ref.close()
