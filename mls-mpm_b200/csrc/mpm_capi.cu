@@ -174,6 +174,11 @@ static bool buffer_info(Scene& s, mpm_buffer which, void** ptr, size_t* bytes) {
     return false;
 }
 
+// The buffers the deferred diffuse tail writes (the pool, its free list and top).
+static bool is_diffuse_buffer(mpm_buffer w) {
+    return w == MPM_BUF_DIFFUSE || w == MPM_BUF_FREE_LIST || w == MPM_BUF_FREE_TOP;
+}
+
 static bool is_particle_buffer(mpm_buffer w) {
     return w == MPM_BUF_POS || w == MPM_BUF_VEL || w == MPM_BUF_AFFINE || w == MPM_BUF_MASS || w == MPM_BUF_DENSITY;
 }
@@ -648,7 +653,7 @@ mpm_status mpm_get_buffer(mpm_scene* sc, mpm_buffer which, void** dev_ptr, size_
     if (!sc || !dev_ptr || !bytes) return fail(MPM_ERR_INVALID_ARG, "NULL argument");
     if (!buffer_info(sc->s, which, dev_ptr, bytes)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_exported = true;
-    {
+    if (is_diffuse_buffer(which)) {
         DeviceGuard guard(sc->s.device);
         CUDA_TRY(flush_tail(sc->s), "diffuse");
     }
@@ -689,7 +694,7 @@ mpm_status mpm_get_ipc_handle(mpm_scene* sc, mpm_buffer which, void* handle, siz
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (which == MPM_BUF_FREE_TOP) sc->s.diffuse.top_exported = true;
     DeviceGuard guard(sc->s.device);
-    CUDA_TRY(flush_tail(sc->s), "diffuse");
+    if (is_diffuse_buffer(which)) CUDA_TRY(flush_tail(sc->s), "diffuse");
     if (is_particle_buffer(which)) {
         Scene& s = sc->s;
         CUDA_TRY(ensure_reference(s, which), "export");
@@ -717,7 +722,7 @@ mpm_status mpm_download(mpm_scene* sc, mpm_buffer which, void* host_dst, size_t 
     if (!buffer_info(sc->s, which, &p, &sz)) return fail(MPM_ERR_INVALID_ARG, "unknown or disabled buffer");
     if (bytes > sz) return fail(MPM_ERR_INVALID_ARG, "bytes exceeds buffer size");
     DeviceGuard guard(sc->s.device);
-    CUDA_TRY(flush_tail(sc->s), "diffuse");
+    if (is_diffuse_buffer(which)) CUDA_TRY(flush_tail(sc->s), "diffuse");
     CUDA_TRY(ensure_reference(sc->s, which), "export");
     CUDA_TRY(cudaMemcpyAsync(host_dst, p, bytes, cudaMemcpyDeviceToHost, sc->s.stream), "download");
     CUDA_TRY(cudaStreamSynchronize(sc->s.stream), "download sync");

@@ -544,14 +544,15 @@ __device__ __forceinline__ int32_t encode_unclamped(float v) { return __float2in
 // paired product feeding scalar adds, or scalar products feeding a paired
 // add, stay separately rounded).  pmul: paired product; smul: two scalar
 // products as a pair; padd: paired add (operands never from pmul); sadd: two
-// scalar adds (for a pmul operand).  MPM_G2P_PACKED / MPM_MOM_PACKED turn
-// the paired forms on per kernel.
+// scalar adds (for a pmul operand).  MPM_G2P_PACKED / MPM_MOM_PACKED select
+// the paired forms per kernel (on by default; 0 builds the scalar forms,
+// which give the same bits).
 // ---------------------------------------------------------------------------
 #ifndef MPM_G2P_PACKED
-#define MPM_G2P_PACKED 0
+#define MPM_G2P_PACKED 1
 #endif
 #ifndef MPM_MOM_PACKED
-#define MPM_MOM_PACKED 0
+#define MPM_MOM_PACKED 1
 #endif
 #if MPM_G2P_PACKED || MPM_MOM_PACKED
 __device__ __forceinline__ unsigned long long pk2(float a, float b) {
