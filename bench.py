@@ -338,6 +338,15 @@ def main():
         roofline["issue_active"] = issue
         roofline["issue_note"] = ("fraction of issue slots used, from the committed ncu summary: the particle "
                                   "kernels are issue/latency-bound, not HBM-bound")
+    # issue roofline: the kernel's warp instructions (committed ncu summary)
+    # against 4 issue slots per SM per clock over its live launch time
+    winst = _profile_value("warp_inst_per_launch", dom, args.workload)
+    csum = clocks.summary()
+    if winst is not None and csum.get("sm_mhz"):
+        props = torch.cuda.get_device_properties(local)
+        slots = 4.0 * props.multi_processor_count * csum["sm_mhz"] * 1e6 * phase_ms[dom] * 1e-3
+        roofline["issue_roofline"] = {"warp_instructions": winst, "issue_slots": slots, "frac": winst / slots,
+                                      "note": "warp instructions / (4 x SMs x median SM clock x live launch time)"}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sub_ms, "higher_is_better": True, "scaling": "weak",

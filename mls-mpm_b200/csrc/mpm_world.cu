@@ -551,6 +551,9 @@ __device__ __forceinline__ int32_t encode_unclamped(float v) { return __float2in
 #ifndef MPM_G2P_PACKED
 #define MPM_G2P_PACKED 1
 #endif
+#ifndef MPM_MIRROR_CS
+#define MPM_MIRROR_CS 0
+#endif
 #ifndef MPM_MOM_PACKED
 #define MPM_MOM_PACKED 1
 #endif
@@ -589,6 +592,22 @@ __device__ __forceinline__ float2 sadd(float2 a, float2 b) { return make_float2(
 // same-cell lanes with a warp reduction first was measured 5x slower.)
 __device__ __forceinline__ uint32_t chunk_lane_offset() {
     return (threadIdx.x & 31u) * (kChunkThreads / 32) + (threadIdx.x >> 5);
+}
+
+// Position within a chunk of kC particles of this thread's particle in pass
+// r.  MPM_P2G_SPREAD: a thread's passes take neighbouring particles and the
+// lanes of a warp spread over the whole chunk, so in dense cells fewer lanes
+// of one shared atomic share its address (results do not depend on it).
+#ifndef MPM_P2G_SPREAD
+#define MPM_P2G_SPREAD 0
+#endif
+template <uint32_t kC>
+__device__ __forceinline__ uint32_t chunk_slot(int r) {
+#if MPM_P2G_SPREAD
+    return (uint32_t)r + (kC / kChunkThreads) * chunk_lane_offset();
+#else
+    return (uint32_t)r * kChunkThreads + chunk_lane_offset();
+#endif
 }
 
 struct ChunkHdr {
@@ -772,7 +791,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
         float4 q[kPer];
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
-            const uint32_t p = h.first + r * kChunkThreads + chunk_lane_offset();
+            const uint32_t p = h.first + chunk_slot<kC>(r);
             q[r] = p < h.end ? posm[v.perm[p]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
         load_scene(v, h.scene, ssd, cached);
@@ -780,7 +799,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
         const SceneDesc& sd = ssd;
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
-            const bool valid = h.first + r * kChunkThreads + chunk_lane_offset() < h.end;
+            const bool valid = h.first + chunk_slot<kC>(r) < h.end;
             const PW w = particle_weights(q[r].x, q[r].y, q[r].z);
             const bool fast = valid && in_halo(w, h, sd);
             const int hb = halo_base(h, w.cx, w.cy, w.cz);
@@ -1350,7 +1369,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
     __syncthreads();
     stage_masses_async(v, hdr[0], cmf, mh[0]);
     // the first particle's inputs
-    uint32_t p = hdr[0].first + chunk_lane_offset();
+    uint32_t p = hdr[0].first + chunk_slot<kC>(0);
     bool valid = p < hdr[0].end;
     float4 pm = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vi = pm;
     float a[9];
@@ -1380,10 +1399,10 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
             uint32_t pn;
             bool vn;
             if (r + 1 < kPer) {
-                pn = p + kChunkThreads;
+                pn = p + (chunk_slot<kC>(1) - chunk_slot<kC>(0));   // the pass stride
                 vn = pn < h.end;
             } else {
-                pn = next_first + chunk_lane_offset();
+                pn = next_first + chunk_slot<kC>(0);
                 vn = has_next && pn < next_end;
             }
             float4 pmn = make_float4(0.0f, 0.0f, 0.0f, 0.0f), vin = pmn;
@@ -1651,9 +1670,17 @@ __device__ __forceinline__ uint32_t g2p_store(const G2POut& o, const SceneDesc& 
     if (mirror) {   // particle_pos/vel (shaders.js:703-704) and particle_density (shaders.js:314) by id
         const uint32_t id = __float_as_uint(vi.w) - sd.id_base;
         if (id < sd.n) {
+#if MPM_MIRROR_CS
+            // streaming stores: the consumer reads these after the step, so they
+            // need not hold L2 lines the next passes use
+            __stcs(ro.pos + id, make_float4(np.x, np.y, np.z, 0.0f));
+            __stcs(ro.vel + id, make_float4(nv.x, nv.y, nv.z, 0.0f));
+            __stcs(ro.dens + id, density);
+#else
             ro.pos[id] = make_float4(np.x, np.y, np.z, 0.0f);
             ro.vel[id] = make_float4(nv.x, nv.y, nv.z, 0.0f);
             ro.dens[id] = density;
+#endif
         }
     }
     // binning of the new position
