@@ -206,6 +206,25 @@ __global__ void k_export(WorldView v, const float4* __restrict__ posm, const flo
     }
 }
 
+// The render mirrors of one scene (particle_pos, particle_vel and
+// particle_density by id) from the substep's new state, as a pass of its own
+// after G2P (MPM_MIRROR_PASS) instead of inside G2P's epilogue.
+__global__ void k_render_export(WorldView v, const float4* __restrict__ posm, const float4* __restrict__ velid,
+                                const float* __restrict__ dens, RefOut ro) {
+    const uint32_t total = min(v.ctrl->total_pos, v.npos);
+    const SceneDesc& sd = v.scenes[ro.scene];
+    const uint32_t id0 = sd.id_base, n = sd.n;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+        const float4 vv = velid[j];
+        const uint32_t id = __float_as_uint(vv.w) - id0;
+        if (id >= n) continue;
+        const float4 p = posm[j];
+        ro.pos[id] = make_float4(p.x, p.y, p.z, 0.0f);
+        ro.vel[id] = make_float4(vv.x, vv.y, vv.z, 0.0f);
+        ro.dens[id] = dens[j];
+    }
+}
+
 // Sets the layout size after imports/removals done outside a substep.
 __global__ void k_set_total(Ctrl* ctrl, uint32_t total) {
     ctrl->total_pos = total;
@@ -2368,6 +2387,10 @@ static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro, bool t
                                                                             w.aff[cur], w.cmf, mv, w.dens);
         w.launches++;
     }
+#ifndef MPM_MIRROR_PASS
+#define MPM_MIRROR_PASS 0
+#endif
+    const RefOut ro_g2p = MPM_MIRROR_PASS ? RefOut{} : ro;   // the mirror inside G2P or as its own pass
     // the tail's ADVECT reads vel4 and its spawn pass the spawn bits that
     // UPDATE_GRID and G2P are about to rewrite
     if (tail_in) {
@@ -2386,11 +2409,15 @@ static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro, bool t
         if (w.chunk == kChunkSmall)
             k_g2p_chunks<kChunkSmall><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4,
                                                                              w.cmf, w.posm[nxt], w.velid[nxt],
-                                                                             w.aff[nxt], dv, ro);
+                                                                             w.aff[nxt], dv, ro_g2p);
         else
             k_g2p_chunks<kChunk><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4,
                                                                         w.cmf, w.posm[nxt], w.velid[nxt],
-                                                                        w.aff[nxt], dv, ro);
+                                                                        w.aff[nxt], dv, ro_g2p);
+        w.launches++;
+    }
+    if (MPM_MIRROR_PASS && ro.enabled) {
+        k_render_export<<<nposb, 256, 0, st>>>(v, w.posm[nxt], w.velid[nxt], w.dens, ro);
         w.launches++;
     }
     w.cur = nxt;
