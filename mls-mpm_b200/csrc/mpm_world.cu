@@ -206,25 +206,6 @@ __global__ void k_export(WorldView v, const float4* __restrict__ posm, const flo
     }
 }
 
-// The render mirrors of one scene (particle_pos, particle_vel and
-// particle_density by id) from the substep's new state, as a pass of its own
-// after G2P (MPM_MIRROR_PASS) instead of inside G2P's epilogue.
-__global__ void k_render_export(WorldView v, const float4* __restrict__ posm, const float4* __restrict__ velid,
-                                const float* __restrict__ dens, RefOut ro) {
-    const uint32_t total = min(v.ctrl->total_pos, v.npos);
-    const SceneDesc& sd = v.scenes[ro.scene];
-    const uint32_t id0 = sd.id_base, n = sd.n;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
-        const float4 vv = velid[j];
-        const uint32_t id = __float_as_uint(vv.w) - id0;
-        if (id >= n) continue;
-        const float4 p = posm[j];
-        ro.pos[id] = make_float4(p.x, p.y, p.z, 0.0f);
-        ro.vel[id] = make_float4(vv.x, vv.y, vv.z, 0.0f);
-        ro.dens[id] = dens[j];
-    }
-}
-
 // Sets the layout size after imports/removals done outside a substep.
 __global__ void k_set_total(Ctrl* ctrl, uint32_t total) {
     ctrl->total_pos = total;
@@ -610,17 +591,6 @@ __device__ __forceinline__ uint32_t chunk_lane_offset() {
     return (threadIdx.x & 31u) * (kChunkThreads / 32) + (threadIdx.x >> 5);
 }
 
-// Copies of the P2G shared accumulators: lane l adds into copy l mod
-// kAccCopies and the flush sums the copies (integer adds commute, so the bits
-// do not change).  Lanes in one cell then rarely hit one address at once.
-#ifndef MPM_ACC_COPIES
-#define MPM_ACC_COPIES 1
-#endif
-constexpr int kAccCopies = MPM_ACC_COPIES;
-__device__ __forceinline__ int acc_copy() { return (int)(threadIdx.x & 31u) % kAccCopies; }
-// P2G_MOM's accumulators (3 components per copy) live in dynamic shared memory
-constexpr size_t kMomAccBytes = kAccCopies > 1 ? sizeof(int32_t) * 3 * kAccCopies * kHaloCells : 0;
-
 // Position within a chunk of kC particles of this thread's particle in pass
 // r.  MPM_P2G_SPREAD (default): a thread's passes take neighbouring particles
 // and the lanes of a warp spread over the whole chunk, so in dense cells fewer
@@ -792,8 +762,7 @@ template <uint32_t kC>
 __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, const float4* __restrict__ posm,
                                                                    int32_t* __restrict__ cm) {
     constexpr int kPer = kC / kChunkThreads;
-    __shared__ int32_t accs[kAccCopies][kHaloCells];
-    int32_t* acc = accs[acc_copy()];   // this lane's copy of the accumulators
+    __shared__ int32_t acc[kHaloCells];
     const uint32_t nch = v.ctrl->total_chunks;
     __shared__ ChunkHdr hs;
     __shared__ SceneDesc ssd;
@@ -804,7 +773,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     if (threadIdx.x == 0 && blockIdx.x < nch)
         chunk_header_from(v.chunk_info[blockIdx.x], v.chunk_last[blockIdx.x], v.chunk_geo[blockIdx.x], hs);
     // the accumulators start at zero and every flush zeroes what it read
-    for (int i = threadIdx.x; i < kAccCopies * kHaloCells; i += blockDim.x) accs[i / kHaloCells][i % kHaloCells] = 0;
+    for (int i = threadIdx.x; i < kHaloCells; i += blockDim.x) acc[i] = 0;
     __syncthreads();
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         const ChunkHdr h = hs;
@@ -867,17 +836,11 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
         if (threadIdx.x == 0 && nxt < nch) chunk_header_from(nci, nlast, ngeo, hs);
         int32_t* scm = cm + sd.cell_base;
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
-            int32_t a = accs[0][i];
-#pragma unroll
-            for (int c = 1; c < kAccCopies; ++c) a = (int32_t)((uint32_t)a + (uint32_t)accs[c][i]);   // wrapping, as the grid
-            bool any = a != 0;
-#pragma unroll
-            for (int c = 1; c < kAccCopies; ++c) any |= accs[c][i] != 0;
-            if (!any) continue;
-#pragma unroll
-            for (int c = 0; c < kAccCopies; ++c) accs[c][i] = 0;
+            const int32_t a = acc[i];
+            if (a == 0) continue;
+            acc[i] = 0;
             uint32_t cell;
-            if (a != 0 && halo_cell(h, sd, i, cell)) atomicAdd(&scm[cell], a);
+            if (halo_cell(h, sd, i, cell)) atomicAdd(&scm[cell], a);
         }
         __syncthreads();
     }
@@ -1383,18 +1346,9 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
                                                                    float* __restrict__ dens) {
     constexpr int kPer = kC / kChunkThreads;
     __shared__ float mh[2][kHaloCells];
+    __shared__ int32_t acc[3][kHaloCells];
     __shared__ ChunkHdr hdr[2];
     __shared__ SceneDesc ssd;
-#if MPM_ACC_COPIES > 1
-    // kAccCopies x 3 components of i32 accumulators (dynamic shared memory:
-    // kMomAccBytes), this lane's copy at acc
-    extern __shared__ __align__(16) int32_t mom_dyn[];
-    int32_t (*accs)[kHaloCells] = reinterpret_cast<int32_t (*)[kHaloCells]>(mom_dyn);
-    int32_t (*acc)[kHaloCells] = accs + 3 * acc_copy();
-#else
-    __shared__ int32_t accs[3][kHaloCells];
-    int32_t (*acc)[kHaloCells] = accs;
-#endif
     const uint32_t nch = v.ctrl->total_chunks;
     const uint32_t G = gridDim.x;
     if (blockIdx.x >= nch) return;   // block-uniform
@@ -1406,15 +1360,11 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
         hdr[0] = unpack_header(v.chunk_hdr[2ull * c0], v.chunk_hdr[2ull * c0 + 1]);
         if (c1 < nch) hdr[1] = unpack_header(v.chunk_hdr[2ull * c1], v.chunk_hdr[2ull * c1 + 1]);
     }
-#if MPM_ACC_COPIES > 1
-    for (int i = threadIdx.x; i < 3 * kAccCopies * kHaloCells; i += blockDim.x) accs[i / kHaloCells][i % kHaloCells] = 0;
-#else
     for (int i = threadIdx.x; i < kHaloCells; i += blockDim.x) {
-        accs[0][i] = 0;
-        accs[1][i] = 0;
-        accs[2][i] = 0;
+        acc[0][i] = 0;
+        acc[1][i] = 0;
+        acc[2][i] = 0;
     }
-#endif
     __syncthreads();
     stage_masses_async(v, hdr[0], cmf, mh[0]);
     // the first particle's inputs
@@ -1470,27 +1420,11 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
         if (threadIdx.x == 0 && nxt2 < nch) hdr[b] = unpack_header(nh0, nh1);
         const int hn = halo_span(h);
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
-#if MPM_ACC_COPIES > 1
-            int32_t a0 = accs[0][i], a1 = accs[1][i], a2 = accs[2][i];
-            uint32_t any = (uint32_t)(a0 | a1 | a2);
-#pragma unroll
-            for (int c = 1; c < kAccCopies; ++c) {   // wrapping adds, as the grid's atomics
-                const int32_t b0 = accs[3 * c][i], b1 = accs[3 * c + 1][i], b2 = accs[3 * c + 2][i];
-                any |= (uint32_t)(b0 | b1 | b2);
-                a0 = (int32_t)((uint32_t)a0 + (uint32_t)b0);
-                a1 = (int32_t)((uint32_t)a1 + (uint32_t)b1);
-                a2 = (int32_t)((uint32_t)a2 + (uint32_t)b2);
-            }
-            if (any == 0) continue;
-#pragma unroll
-            for (int c = 0; c < 3 * kAccCopies; ++c) accs[c][i] = 0;
-#else
-            const int32_t a0 = accs[0][i], a1 = accs[1][i], a2 = accs[2][i];
+            const int32_t a0 = acc[0][i], a1 = acc[1][i], a2 = acc[2][i];
             if ((a0 | a1 | a2) == 0) continue;
-            accs[0][i] = 0;
-            accs[1][i] = 0;
-            accs[2][i] = 0;
-#endif
+            acc[0][i] = 0;
+            acc[1][i] = 0;
+            acc[2][i] = 0;
             uint32_t cell;
             if (halo_cell(h, sd, i, cell)) {
                 int32_t* d = smv + 3ull * cell;
@@ -2031,12 +1965,6 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
     w.scenes.assign(scene_cap, SceneRec());
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    // P2G_MOM's accumulator copies may pass the 48 KB default of dynamic shared memory
-    if (kMomAccBytes > 32 * 1024) {
-        cudaFuncSetAttribute(k_p2g_mom_chunks<kChunk>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMomAccBytes);
-        cudaFuncSetAttribute(k_p2g_mom_chunks<kChunkSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kMomAccBytes);
-    }
     w.sms = (uint32_t)sms;
     w.item_blocks = (uint32_t)sms * 4;
     w.grid_blocks = (uint32_t)sms * 8;
@@ -2380,17 +2308,13 @@ static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro, bool t
     {
         Phase ph(prof, MPM_PHASE_P2G_MOM);
         if (w.chunk == kChunkSmall)
-            k_p2g_mom_chunks<kChunkSmall><<<w.item_blocks, kChunkThreads, kMomAccBytes, st>>>(v, w.posm[cur], w.velid[cur],
+            k_p2g_mom_chunks<kChunkSmall><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur],
                                                                                  w.aff[cur], w.cmf, mv, w.dens);
         else
-            k_p2g_mom_chunks<kChunk><<<w.item_blocks, kChunkThreads, kMomAccBytes, st>>>(v, w.posm[cur], w.velid[cur],
+            k_p2g_mom_chunks<kChunk><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur],
                                                                             w.aff[cur], w.cmf, mv, w.dens);
         w.launches++;
     }
-#ifndef MPM_MIRROR_PASS
-#define MPM_MIRROR_PASS 0
-#endif
-    const RefOut ro_g2p = MPM_MIRROR_PASS ? RefOut{} : ro;   // the mirror inside G2P or as its own pass
     // the tail's ADVECT reads vel4 and its spawn pass the spawn bits that
     // UPDATE_GRID and G2P are about to rewrite
     if (tail_in) {
@@ -2409,15 +2333,11 @@ static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro, bool t
         if (w.chunk == kChunkSmall)
             k_g2p_chunks<kChunkSmall><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4,
                                                                              w.cmf, w.posm[nxt], w.velid[nxt],
-                                                                             w.aff[nxt], dv, ro_g2p);
+                                                                             w.aff[nxt], dv, ro);
         else
             k_g2p_chunks<kChunk><<<w.item_blocks, kChunkThreads, 0, st>>>(v, w.posm[cur], w.velid[cur], w.vel4,
                                                                         w.cmf, w.posm[nxt], w.velid[nxt],
-                                                                        w.aff[nxt], dv, ro_g2p);
-        w.launches++;
-    }
-    if (MPM_MIRROR_PASS && ro.enabled) {
-        k_render_export<<<nposb, 256, 0, st>>>(v, w.posm[nxt], w.velid[nxt], w.dens, ro);
+                                                                        w.aff[nxt], dv, ro);
         w.launches++;
     }
     w.cur = nxt;
