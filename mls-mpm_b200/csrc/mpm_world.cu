@@ -583,10 +583,12 @@ __device__ __forceinline__ float2 sadd(float2 a, float2 b) { return make_float2(
 // ---------------------------------------------------------------------------
 // Chunks: the halo box of a chunk's cells in shared memory
 // ---------------------------------------------------------------------------
-// Lane layout of the P2G chunk kernels: within each pass over the chunk, lane
-// l of warp w takes particle 8*l + w, so neighbouring lanes sit in different
-// cells and the lanes of one shared atomic rarely share an address.  (Adding
-// same-cell lanes with a warp reduction first was measured 5x slower.)
+// Lane order of the P2G chunk kernels: lane l of warp w has offset 8*l + w
+// (8 warps per block), which chunk_slot scales to a particle of the chunk, so
+// neighbouring lanes sit in different cells and the lanes of one shared
+// atomic rarely share an address.  (Adding same-cell lanes with a warp
+// reduction first was measured slower, both per cell with match + redux and
+// for warp passes in at most two cells.)
 __device__ __forceinline__ uint32_t chunk_lane_offset() {
     return (threadIdx.x & 31u) * (kChunkThreads / 32) + (threadIdx.x >> 5);
 }
