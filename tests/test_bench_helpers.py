@@ -18,13 +18,16 @@ def test_l2_note_sizes_the_working_set():
 
 
 def test_profile_lookups_follow_the_workload():
-    # the committed capture of the 1M dam break carries traffic and issue use
-    # of the dominant kernel; other workloads have none
+    # the committed captures of the 1M and 8M dam breaks carry traffic and
+    # issue use of the dominant kernel (below its algorithmic bytes: 113.2 MB
+    # and 771.8 MB per launch); a workload without a capture has none
     t = bench._profile_traffic("p2g_mom", "dam_break_1m")
     assert isinstance(t, int) and 50_000_000 < t < 113_246_208
     issue = bench._profile_value("issue_active_per_launch", "p2g_mom", "dam_break_1m")
     assert 0.0 < issue <= 1.0
-    assert bench._profile_traffic("p2g_mom", "dam_break_sphere_8m") is None
+    t8 = bench._profile_traffic("p2g_mom", "dam_break_sphere_8m")
+    assert isinstance(t8, int) and 400_000_000 < t8 < 771_751_936
+    assert bench._profile_traffic("p2g_mom", "dam_break_64") is None
     assert bench._profile_traffic("no_such_phase", "dam_break_1m") is None
 
 
