@@ -100,7 +100,7 @@ WorldView World::view() const {
     if (v.ngroups == 0) v.ngroups = 1;
     v.chunk_cap = chunk_cap;
     v.chunk = chunk;
-    v.scenes = d_scenes;
+    v.scenes = scenes_dev(cur);
     v.tile_scene = tile_scene;
     v.cell_count = cell_count; v.cell_start = cell_start;
     v.key = key; v.rank = rank; v.perm = perm;
@@ -1941,7 +1941,7 @@ template <class F> static void world_arrays(World& w, F&& f) {
     f(w.cmf, C * 4);
     f(w.mvf, C * 12);
     f(w.vel4, C * 16);
-    f(w.d_scenes, (size_t)w.scene_cap * sizeof(SceneDesc));
+    f(w.d_scenes, 2 * (size_t)w.scene_cap * sizeof(SceneDesc));
     f(w.health, (size_t)(w.scene_cap ? w.scene_cap : 1) * 4);
 }
 
@@ -1984,7 +1984,10 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
         e = cudaMallocHost((void**)&w.h_stage[b], (size_t)scene_cap * sizeof(SceneDesc));
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.stage_ev[b], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.sub_done[b], cudaEventDisableTiming);
     }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w.tbl_side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.tbl_ev, cudaEventDisableTiming);
     if (e != cudaSuccess) return e;
     w.h_tile_scene.assign(T, kHole);
     // zero everything the sparse passes rely on being zero
@@ -2010,12 +2013,17 @@ cudaError_t world_alloc(World& w, int device, cudaStream_t stream, uint32_t part
 
 void world_free(World& w) {
     if (w.stream) cudaStreamSynchronize(w.stream);
+    if (w.tbl_side) cudaStreamSynchronize(w.tbl_side);
     for (int b = 0; b < 2; ++b) {
         if (w.h_stage[b]) cudaFreeHost(w.h_stage[b]);
         if (w.stage_ev[b]) cudaEventDestroy(w.stage_ev[b]);
+        if (w.sub_done[b]) cudaEventDestroy(w.sub_done[b]);
         w.h_stage[b] = nullptr;
         w.stage_ev[b] = nullptr;
+        w.sub_done[b] = nullptr;
     }
+    if (w.tbl_ev) cudaEventDestroy(w.tbl_ev);
+    if (w.tbl_side) cudaStreamDestroy(w.tbl_side);
     for (int b = 0; b < World::kGraphs; ++b)
         if (w.graph[b]) cudaGraphExecDestroy(w.graph[b]);
     world_arrays(w, [](auto*& p, size_t) {
@@ -2046,27 +2054,77 @@ static void fill_desc(World& w, int slot) {
     d.H = r.H;
 }
 
-cudaError_t world_upload_table(World& w) {
-    if (!w.table_dirty) return cudaSuccess;
+static int table_entries(const World& w) {
     int hi = 0;
     for (int i = 0; i < (int)w.scene_cap; ++i)
         if (w.scenes[i].live) hi = i + 1;
+    return hi;
+}
+
+// The host table from the scene records, when they changed: both device
+// copies are then behind.
+static void refresh_host_table(World& w) {
+    if (!w.table_dirty) return;
+    const int hi = table_entries(w);
     for (int i = 0; i < hi; ++i) fill_desc(w, i);
+    w.table_dirty = false;
+    w.tbl_dirty[0] = w.tbl_dirty[1] = true;
+}
+
+// Copies the host table into device copy c on stream st, through pinned
+// staging (an upload from pageable memory would first wait for all work
+// queued on the stream); a staging buffer is reused only once the copy that
+// last read it has run.
+static cudaError_t upload_copy(World& w, int c, cudaStream_t st) {
+    const int hi = table_entries(w);
     cudaError_t e = cudaSuccess;
     if (hi) {
-        // pinned staging copy (an upload from pageable memory would first wait
-        // for all work queued on the stream); the copy it last fed must be done
         const int b = w.stage_i;
         w.stage_i ^= 1;
         e = cudaEventSynchronize(w.stage_ev[b]);
         if (e == cudaSuccess) {
             std::memcpy(w.h_stage[b], w.h_scenes.data(), (size_t)hi * sizeof(SceneDesc));
-            e = cudaMemcpyAsync(w.d_scenes, w.h_stage[b], (size_t)hi * sizeof(SceneDesc), cudaMemcpyHostToDevice,
-                                w.stream);
+            e = cudaMemcpyAsync(w.scenes_dev(c), w.h_stage[b], (size_t)hi * sizeof(SceneDesc),
+                                cudaMemcpyHostToDevice, st);
         }
-        if (e == cudaSuccess) e = cudaEventRecord(w.stage_ev[b], w.stream);
+        if (e == cudaSuccess) e = cudaEventRecord(w.stage_ev[b], st);
     }
-    if (e == cudaSuccess) w.table_dirty = false;
+    if (e == cudaSuccess) w.tbl_dirty[c] = false;
+    return e;
+}
+
+// Outside a substep: both copies in stream order, so the kernels about to be
+// launched and every later substep see the current table.
+cudaError_t world_upload_table(World& w) {
+    refresh_host_table(w);
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < 2 && e == cudaSuccess; ++c)
+        if (w.tbl_dirty[c]) {
+            e = upload_copy(w, c, w.stream);
+            if (e == cudaSuccess) w.tbl_outside[c] = false;
+        }
+    return e;
+}
+
+// Before a substep of parity cur: its copy of the table.  When nothing but
+// the substep two back (same parity) has read that copy since it was last
+// written, the copy is made on a side stream after that substep, beside the
+// substep now running, and this one waits for it; a copy made between two
+// substeps in stream order would leave the GPU idle for its round trip
+// (uniforms change every frame: the hand, walls).
+static cudaError_t upload_table_for_substep(World& w) {
+    refresh_host_table(w);
+    const int c = w.cur;
+    if (!w.tbl_dirty[c]) return cudaSuccess;
+    if (w.tbl_outside[c]) {
+        const cudaError_t e = upload_copy(w, c, w.stream);
+        if (e == cudaSuccess) w.tbl_outside[c] = false;
+        return e;
+    }
+    cudaError_t e = cudaStreamWaitEvent(w.tbl_side, w.sub_done[c], 0);
+    if (e == cudaSuccess) e = upload_copy(w, c, w.tbl_side);
+    if (e == cudaSuccess) e = cudaEventRecord(w.tbl_ev, w.tbl_side);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(w.stream, w.tbl_ev, 0);
     return e;
 }
 
@@ -2142,6 +2200,7 @@ cudaError_t world_add_scene(World& w, uint32_t X, uint32_t Y, uint32_t Z, const 
                                                      w.posm[w.cur], w.velid[w.cur], w.aff[w.cur], n);
         k_set_total<<<1, 1, 0, w.stream>>>(w.ctrl, h_total + n);
         w.launches += 3;
+        w.tbl_outside[w.cur] = true;
         // the other positions keep the ranks G2P counted: count only the new
         // ones (before any count, the next substep counts everything)
         if (w.counted) {
@@ -2181,6 +2240,7 @@ cudaError_t world_remove_scene(World& w, int slot) {
     if (r.n) {
         k_remove<<<w.pos_blocks, 256, 0, w.stream>>>(v, w.velid[w.cur], r.id_base, r.n);
         w.launches++;
+        w.tbl_outside[w.cur] = true;
     }
     // zero the scene's grid region (both i32 buffers, decoded mirrors) and free its ranges
     cudaError_t e = cudaSuccess;
@@ -2224,6 +2284,7 @@ cudaError_t world_export_scene(World& w, int slot, float4* pos, float4* vel, flo
                                                       r.id_base, r.n, pos, vel, aff, mass,
                                                       w.dens_valid ? dens : nullptr);
     w.launches++;
+    w.tbl_outside[w.cur] = true;
     return cudaGetLastError();
 }
 
@@ -2352,7 +2413,7 @@ static cudaError_t enqueue_substep(World& w, Scene* ds, const RefOut& ro, bool t
     if (e != cudaSuccess) return e;
     if (dv.enabled) {
         ds->diffuse.seed += 1u;   // mirrors the device-side bump in k_tile_scan_top
-        const SceneDesc* sd_dev = w.d_scenes + dv.scene;
+        const SceneDesc* sd_dev = w.scenes_dev(cur) + dv.scene;
         if (defer) {
             // this substep's uniforms for its deferred tail (the scene table may
             // be rewritten before the tail runs)
@@ -2391,8 +2452,9 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
         w.chunk = chunk;
         w.generation++;
     }
-    cudaError_t e = world_upload_table(w);
+    cudaError_t e = upload_table_for_substep(w);
     if (e != cudaSuccess) return e;
+    const int parity = w.cur;   // the table copy this substep reads
     const bool diffuse = ds && ds->diffuse.enabled;
     const bool profiling = ds && ds->profile;
     if (profiling && diffuse && ds->diffuse.tail_pending) {
@@ -2403,7 +2465,11 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
     const bool tail_in = diffuse && ds->diffuse.tail_pending;
     const bool defer = diffuse && !profiling;
     // a substep that must recount runs eagerly; the captured graphs never count
-    if (!use_graph || profiling || !w.counted) return enqueue_substep(w, ds, ro, tail_in, defer);
+    if (!use_graph || profiling || !w.counted) {
+        e = enqueue_substep(w, ds, ro, tail_in, defer);
+        if (e == cudaSuccess) e = cudaEventRecord(w.sub_done[parity], w.stream);
+        return e;
+    }
     // the diffuse update joins the graph: its kernels read the uniforms from
     // device copies and the advect parameters from a device copy
     Scene* dsc = diffuse ? ds : nullptr;
@@ -2455,6 +2521,7 @@ cudaError_t world_substep(World& w, Scene* ds, bool use_graph) {
         w.graph_mirror[p] = mirror;
     }
     e = cudaGraphLaunch(w.graph[p], w.stream);
+    if (e == cudaSuccess) e = cudaEventRecord(w.sub_done[parity], w.stream);
     if (e != cudaSuccess) return e;
     // host mirror of what the graph does
     w.launches += w.graph_kernels[p];

@@ -172,7 +172,17 @@ struct World {
     uint64_t generation = 1;                // bumps whenever the captured launch arguments change
 
     // device arrays
-    SceneDesc* d_scenes = nullptr;
+    // the device scene table, one copy per buffer parity: a substep of
+    // parity c, and every kernel launched while cur == c, reads copy c
+    // (d_scenes + c * scene_cap), so a copy can be rewritten while the
+    // substep of the other parity runs
+    SceneDesc* d_scenes = nullptr;          // 2 * scene_cap entries
+    bool tbl_dirty[2] = {true, true};       // copy c is behind h_scenes
+    bool tbl_outside[2] = {false, false};   // copy c was read outside a substep since its last in-order upload
+    cudaStream_t tbl_side = nullptr;        // table uploads beside the running substep
+    cudaEvent_t sub_done[2] = {nullptr, nullptr};   // after the last substep of each parity
+    cudaEvent_t tbl_ev = nullptr;           // the last upload on tbl_side
+    SceneDesc* scenes_dev(int c) const { return d_scenes + (size_t)c * scene_cap; }
     std::vector<SceneDesc> h_scenes;        // host copy of the table
     // pinned staging copies of the table for asynchronous uploads (a copy from
     // pageable memory would wait for the stream); each is reused only after
