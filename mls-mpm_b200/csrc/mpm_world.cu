@@ -681,18 +681,27 @@ __device__ __forceinline__ ChunkHdr unpack_header(const uint4 a, const uint4 b) 
     return h;
 }
 
-// The chunk's scene descriptor in shared memory (copied when the scene
-// changes from the block's previous chunk), so per-particle reads of grid
-// dims and uniforms are shared-memory loads.  Block-uniform: every thread
-// calls it right after the chunk header is visible; `cached` is per thread.
-__device__ __forceinline__ void load_scene(const WorldView& v, uint32_t scene, SceneDesc& ssd, uint32_t& cached) {
-    static_assert(sizeof(SceneDesc) % 16 == 0, "SceneDesc copy in 16-byte words");
-    if (scene == cached) return;
-    const uint4* src = reinterpret_cast<const uint4*>(v.scenes + scene);
-    uint4* dst = reinterpret_cast<uint4*>(&ssd);
-    for (int i = threadIdx.x; i < (int)(sizeof(SceneDesc) / 16); i += blockDim.x) dst[i] = src[i];
-    __syncthreads();
-    cached = scene;
+// Each block of the chunk kernels keeps its chunk's scene descriptor in
+// shared memory, so per-particle reads of grid dims and uniforms are shared
+// loads; the next chunk's descriptor is copied while the current one runs.
+static_assert(sizeof(SceneDesc) % 16 == 0, "SceneDesc copy in 16-byte words");
+
+// Starts copying scene `scene`'s descriptor into shared memory (cp.async,
+// 16-byte words); the block's next cp_async_wait and barrier make it visible.
+__device__ __forceinline__ void copy_scene_async(const WorldView& v, uint32_t scene, SceneDesc& dst) {
+    constexpr int kWords = (int)(sizeof(SceneDesc) / 16);
+    if (threadIdx.x < kWords)
+        cp_async16(reinterpret_cast<uint4*>(&dst) + threadIdx.x, reinterpret_cast<const uint4*>(v.scenes + scene) + threadIdx.x,
+                   16u);
+}
+
+// The same, issued by one thread (36 copies); its own cp_async_wait and the
+// next barrier make it visible.
+__device__ __forceinline__ void copy_scene_async_one(const WorldView& v, uint32_t scene, SceneDesc& dst) {
+    constexpr int kWords = (int)(sizeof(SceneDesc) / 16);
+#pragma unroll 4
+    for (int i = 0; i < kWords; ++i)
+        cp_async16(reinterpret_cast<uint4*>(&dst) + i, reinterpret_cast<const uint4*>(v.scenes + scene) + i, 16u);
 }
 
 // True when the particle's 3x3x3 stencil lies in the chunk's halo box and in
@@ -767,13 +776,20 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
     __shared__ int32_t acc[kHaloCells];
     const uint32_t nch = v.ctrl->total_chunks;
     __shared__ ChunkHdr hs;
-    __shared__ SceneDesc ssd;
-    uint32_t cached = kHole;
+    // scene descriptors of this chunk and the next (thread 0 copies the next
+    // one while this chunk runs)
+    __shared__ SceneDesc ssd[2];
+    int sb = 0;                                      // ssd[sb]: this chunk's scene
+    uint32_t ss_nxt = kHole;                         // thread 0: scene held in ssd[sb ^ 1]
     // thread 0: the next chunk's header words, loaded while this chunk runs
     uint4 nci = make_uint4(0u, 0u, 0u, 0u), ngeo = nci;
     uint32_t nlast = 0;
-    if (threadIdx.x == 0 && blockIdx.x < nch)
-        chunk_header_from(v.chunk_info[blockIdx.x], v.chunk_last[blockIdx.x], v.chunk_geo[blockIdx.x], hs);
+    if (threadIdx.x == 0 && blockIdx.x < nch) {
+        const uint4 g0 = v.chunk_geo[blockIdx.x];
+        chunk_header_from(v.chunk_info[blockIdx.x], v.chunk_last[blockIdx.x], g0, hs);
+        copy_scene_async_one(v, g0.x, ssd[0]);
+        cp_async_wait();
+    }
     // the accumulators start at zero and every flush zeroes what it read
     for (int i = threadIdx.x; i < kHaloCells; i += blockDim.x) acc[i] = 0;
     __syncthreads();
@@ -795,9 +811,8 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             const uint32_t p = h.first + chunk_slot<kC>(r);
             q[r] = p < h.end ? posm[v.perm[p]] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
-        load_scene(v, h.scene, ssd, cached);
         const int hn = halo_span(h);
-        const SceneDesc& sd = ssd;
+        const SceneDesc& sd = ssd[sb];
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
             const bool valid = h.first + chunk_slot<kC>(r) < h.end;
@@ -835,7 +850,13 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
         }
         __syncthreads();
         // every thread holds this chunk's header: the next one can replace it
-        if (threadIdx.x == 0 && nxt < nch) chunk_header_from(nci, nlast, ngeo, hs);
+        if (threadIdx.x == 0 && nxt < nch) {
+            chunk_header_from(nci, nlast, ngeo, hs);
+            if (ngeo.x != ss_nxt) {
+                copy_scene_async_one(v, ngeo.x, ssd[sb ^ 1]);
+                ss_nxt = ngeo.x;
+            }
+        }
         int32_t* scm = cm + sd.cell_base;
         for (int i = threadIdx.x; i < hn; i += blockDim.x) {
             const int32_t a = acc[i];
@@ -844,7 +865,12 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
             uint32_t cell;
             if (halo_cell(h, sd, i, cell)) atomicAdd(&scm[cell], a);
         }
+        if (threadIdx.x == 0) {
+            cp_async_wait();
+            ss_nxt = h.scene;   // after the swap ssd[sb ^ 1] holds this chunk's scene
+        }
         __syncthreads();
+        sb ^= 1;
     }
 }
 
@@ -1350,12 +1376,13 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
     __shared__ float mh[2][kHaloCells];
     __shared__ int32_t acc[3][kHaloCells];
     __shared__ ChunkHdr hdr[2];
-    __shared__ SceneDesc ssd;
+    // the scene descriptors of the current chunk and of the next one, which is
+    // copied while the current chunk runs (no wait when the scene changes)
+    __shared__ SceneDesc ssd[2];
     const uint32_t nch = v.ctrl->total_chunks;
     const uint32_t G = gridDim.x;
     if (blockIdx.x >= nch) return;   // block-uniform
     const size_t plane = v.npos;
-    uint32_t cached = kHole;
     uint4 nh0 = make_uint4(0u, 0u, 0u, 0u), nh1 = nh0;   // thread 0: the words of the chunk two ahead
     if (threadIdx.x == 0) {
         const uint32_t c0 = blockIdx.x, c1 = c0 + G;
@@ -1368,6 +1395,8 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
         acc[2][i] = 0;
     }
     __syncthreads();
+    copy_scene_async(v, hdr[0].scene, ssd[0]);
+    uint32_t ss_cur = hdr[0].scene, ss_nxt = kHole;   // scenes held in ssd[b], ssd[b ^ 1]
     stage_masses_async(v, hdr[0], cmf, mh[0]);
     // the first particle's inputs
     uint32_t p = hdr[0].first + chunk_slot<kC>(0);
@@ -1385,13 +1414,19 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
             nh0 = v.chunk_hdr[2ull * nxt2];
             nh1 = v.chunk_hdr[2ull * nxt2 + 1];
         }
-        load_scene(v, h.scene, ssd, cached);
-        const SceneDesc& sd = ssd;
+        const SceneDesc& sd = ssd[b];
         const float* scmf = cmf + sd.cell_base;
         int32_t* smv = mv + 3ull * sd.cell_base;
-        // the next chunk's halo masses, copied while this chunk runs
+        // the next chunk's halo masses (and scene descriptor), copied while this chunk runs
         const bool has_next = nxt < nch;
-        if (has_next) stage_masses_async(v, hdr[b ^ 1], cmf, mh[b ^ 1]);
+        if (has_next) {
+            stage_masses_async(v, hdr[b ^ 1], cmf, mh[b ^ 1]);
+            const uint32_t ns = hdr[b ^ 1].scene;
+            if (ns != ss_nxt) {
+                copy_scene_async(v, ns, ssd[b ^ 1]);
+                ss_nxt = ns;
+            }
+        }
         const uint32_t next_first = has_next ? hdr[b ^ 1].first : 0u, next_end = has_next ? hdr[b ^ 1].end : 0u;
 #pragma unroll 1
         for (int r = 0; r < kPer; ++r) {
@@ -1438,6 +1473,9 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_MOM_MINB) k_p2g_mom_chunks(
         cp_async_wait();
         __syncthreads();
         b ^= 1;
+        const uint32_t t = ss_cur;
+        ss_cur = ss_nxt;
+        ss_nxt = t;
     }
 }
 
@@ -1771,8 +1809,11 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
     const uint32_t nch = v.ctrl->total_chunks;
     const size_t plane = v.npos;
     __shared__ ChunkHdr hs;
-    __shared__ SceneDesc ssd;
-    uint32_t cached = kHole;
+    // scene descriptors of this chunk and the next (thread 0 copies the next
+    // one while this chunk runs)
+    __shared__ SceneDesc ssd[2];
+    int sb = 0;                 // ssd[sb]: this chunk's scene
+    uint32_t ss_nxt = kHole;    // thread 0: scene held in ssd[sb ^ 1]
     // rank of the last particle whose atomic is still in flight
     uint32_t pend_p = kHole, pend_rank = 0;
     const float bubble_min = dv.enabled ? dv.gen->density_bubble_min : 0.0f;
@@ -1786,7 +1827,11 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         v.ctrl->bins_done = 0u;
     }
     // chunk headers: the next one's words are copied while this chunk runs
-    if (threadIdx.x == 0 && blockIdx.x < nch) hs = unpack_header(v.chunk_hdr[2ull * blockIdx.x], v.chunk_hdr[2ull * blockIdx.x + 1]);
+    if (threadIdx.x == 0 && blockIdx.x < nch) {
+        hs = unpack_header(v.chunk_hdr[2ull * blockIdx.x], v.chunk_hdr[2ull * blockIdx.x + 1]);
+        copy_scene_async_one(v, hs.scene, ssd[0]);
+        cp_async_wait();
+    }
     __syncthreads();
     for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
         const ChunkHdr h = hs;
@@ -1795,8 +1840,7 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
             cp_async16(&nhs[0], v.chunk_hdr + 2ull * nxt, 16u);
             cp_async16(&nhs[1], v.chunk_hdr + 2ull * nxt + 1, 16u);
         }
-        load_scene(v, h.scene, ssd, cached);
-        const SceneDesc& sd = ssd;
+        const SceneDesc& sd = ssd[sb];
         // this thread's particles, in flight while the halo is staged
         float4 qs[kPer];
         float ids[kPer], dns[kPer];
@@ -1826,6 +1870,10 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
         if (threadIdx.x == 0 && nxt < nch) {
             cp_async_wait();
             hs = unpack_header(nhs[0], nhs[1]);
+            if (hs.scene != ss_nxt) {
+                copy_scene_async_one(v, hs.scene, ssd[sb ^ 1]);
+                ss_nxt = hs.scene;
+            }
         }
         const bool spawn_scene = dv.enabled && h.scene == dv.scene;
         const bool mirror = ro.enabled && h.scene == ro.scene;
@@ -1880,7 +1928,12 @@ __global__ void __launch_bounds__(kChunkThreads, MPM_G2P_MINB) k_g2p_chunks(Worl
             pend_p = p;
             pend_rank = rk;
         }
+        if (threadIdx.x == 0) {
+            cp_async_wait();      // the next chunk's scene descriptor
+            ss_nxt = h.scene;     // after the swap ssd[sb ^ 1] holds this chunk's scene
+        }
         __syncthreads();
+        sb ^= 1;
     }
     if (pend_p != kHole) v.rank[pend_p] = pend_rank;
 }
