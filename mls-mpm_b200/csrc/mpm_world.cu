@@ -804,7 +804,7 @@ __global__ void __launch_bounds__(kChunkThreads) k_p2g_mass_chunks(WorldView v, 
                 ngeo = v.chunk_geo[nxt];
             }
         }
-        // this thread's particles, in flight while the scene descriptor loads
+        // this thread's particles, all loads issued before the first is used
         float4 q[kPer];
 #pragma unroll
         for (int r = 0; r < kPer; ++r) {
