@@ -51,6 +51,12 @@
 #include "mpm_scene.h"
 #include "mpm_world.h"
 
+// MPM_MIRROR_KEEP (default): the render mirrors' stores carry an L2
+// evict-last hint (measured: G2P with the mirrors 93.6 -> 85.9 us at 1M).
+#ifndef MPM_MIRROR_KEEP
+#define MPM_MIRROR_KEEP 1
+#endif
+
 namespace mpm {
 
 // ---------------------------------------------------------------------------
@@ -1709,9 +1715,23 @@ __device__ __forceinline__ uint32_t g2p_store(const G2POut& o, const SceneDesc& 
     if (mirror) {   // particle_pos/vel (shaders.js:703-704) and particle_density (shaders.js:314) by id
         const uint32_t id = __float_as_uint(vi.w) - sd.id_base;
         if (id < sd.n) {
+#if MPM_MIRROR_KEEP
+            // the scattered 16- and 4-byte writes by id fill 32-byte sectors
+            // half or an eighth at a time: an evict-last hint keeps their L2
+            // lines until the rest of each sector has been written
+            uint64_t pol;
+            asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+            asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(ro.pos + id), "f"(np.x),
+                         "f"(np.y), "f"(np.z), "f"(0.0f), "l"(pol) : "memory");
+            asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(ro.vel + id), "f"(nv.x),
+                         "f"(nv.y), "f"(nv.z), "f"(0.0f), "l"(pol) : "memory");
+            asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(ro.dens + id), "f"(density), "l"(pol)
+                         : "memory");
+#else
             ro.pos[id] = make_float4(np.x, np.y, np.z, 0.0f);
             ro.vel[id] = make_float4(nv.x, nv.y, nv.z, 0.0f);
             ro.dens[id] = density;
+#endif
         }
     }
     // binning of the new position
